@@ -1,0 +1,198 @@
+/*
+ * hurchem_b200.h -- C ABI of the B200 chemistry source-term library
+ * (libhurchem_b200.so, built from openhurricane_b200/csrc/).
+ *
+ * The library integrates OpenHurricane's chemistry source term on an NVIDIA
+ * B200 (sm_100a): per-cell stiff integration of finite-rate kinetics over
+ * one flow time step with the reference's implicit-Euler scheme in FP64, the
+ * source terms omega_i * W_i, and the NASA-7 / kinetic-theory mixture
+ * properties. Every entry point takes plain pointers and sizes; no CUDA or
+ * torch type appears in a signature (streams are passed as void*).
+ *
+ * Layout: per-cell fields are structure-of-arrays. A species field is
+ * [nsp][ncells] (species-major, cell index fastest), the layout the
+ * reference's flow solver keeps its PtrList<cellRealArray> yi_ in.
+ *
+ * Errors: every function returns an int status: 0 = success, > 0 = number
+ * of cells that ended with a non-OK per-cell status (see HC_CELL_*), < 0 =
+ * fatal (HC_E_*). hc_last_error() returns a message for the last failure on
+ * the calling thread. The library never aborts the host process.
+ *
+ * Ownership: handles (hc_mech_t, hc_workspace_t) own device memory; host
+ * arrays are caller-owned. Calls taking a stream are stream-ordered and
+ * asynchronous unless their name ends in _host, which copies to and from
+ * host memory and synchronises the stream before returning.
+ */
+#ifndef HURCHEM_B200_H
+#define HURCHEM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HC_ABI_VERSION 1
+
+/* fatal status codes */
+#define HC_OK 0
+#define HC_E_INVALID (-1)     /* bad argument (null pointer, size, option) */
+#define HC_E_CUDA (-2)        /* CUDA runtime error */
+#define HC_E_UNSUPPORTED (-3) /* mechanism / option outside the kernel's range */
+#define HC_E_NOMEM (-4)
+
+/* per-cell status words written by the integrators */
+#define HC_CELL_OK 0
+#define HC_CELL_SKIPPED 1       /* T below the temperature threshold: not integrated */
+#define HC_CELL_MAXSTEP 2       /* an ODE solve hit maxstep (the reference then restarts it) */
+#define HC_CELL_UNDERFLOW 4     /* step size fell below 1e-300 (the reference aborts here) */
+#define HC_CELL_ITER_LIMIT 8    /* safety cap on total Newton iterations reached */
+
+/* rate-law codes of hc_mech_desc.rate_type */
+#define HC_RATE_ARRHENIUS 0
+#define HC_RATE_THIRD_BODY 1
+#define HC_RATE_LINDEMANN 2
+#define HC_RATE_TROE3 3
+#define HC_RATE_TROE4 4
+
+#define HC_MAX_SIDE 4
+
+/*
+ * Flattened mechanism (SI units: kg, m, s, kmol, K, J). Produced on the host
+ * from Chemkin / NASA-7 / transport files (openhurricane_b200/mechanism.py
+ * applies the reference's unit conversions). Mirrors the data the reference's
+ * mixture flattens for its GPU path (reactions/cuda/include/cuChemInterface.hpp:39-342),
+ * but structure-of-arrays per reaction.
+ */
+typedef struct hc_mech_desc {
+    int32_t nsp;             /* species */
+    int32_t nrc;             /* reactions */
+    const double *W;         /* [nsp] molecular weights kg/kmol */
+    const double *Trange;    /* [nsp*3] Tlow, Tcommon, Thigh */
+    const double *nasa;      /* [nsp*14] mass-basis NASA-7: low a0..a6, high a0..a6 */
+    const int32_t *rate_type;  /* [nrc] HC_RATE_* */
+    const int32_t *reversible; /* [nrc] 1 reversible, 0 irreversible */
+    const double *arr;       /* [nrc*3] A, beta, Ta (high-pressure limit for fall-off) */
+    const double *arr0;      /* [nrc*3] low-pressure limit (fall-off only) */
+    const double *troe;      /* [nrc*4] alpha, T***, T*, T** */
+    const double *eff;       /* [nrc*nsp] third-body efficiencies */
+    const int32_t *nf;       /* [nrc] reactants */
+    const int32_t *nb;       /* [nrc] products */
+    const int32_t *fidx;     /* [nrc*HC_MAX_SIDE] */
+    const int32_t *bidx;
+    const double *fnu;       /* [nrc*HC_MAX_SIDE] stoichiometric coefficients */
+    const double *bnu;
+    const double *ford;      /* [nrc*HC_MAX_SIDE] reaction orders */
+    const double *bord;
+    /* kinetic-theory transport data (transport/include/kineticTheory.hpp) */
+    const int32_t *geom;     /* [nsp] */
+    const double *eps_k;     /* [nsp] well depth / kB, K */
+    const double *sigma;     /* [nsp] collision diameter, Angstrom */
+} hc_mech_desc;
+
+/*
+ * Integrator options. Names and defaults follow the reference's controller
+ * keys: solver/{maxstep, atol, rtol, safescale, minscale, maxScale, alphainc}
+ * (Hurricane/mathematicalTools/ODEs/src/ODEsSolver.cpp:80-92),
+ * ImplicitEuler/{autoUpdateJacobian, stepToUpdateJac, ATolIncrement,
+ * RTolIncrement} (ODEs/src/ImplicitEuler.cpp:68-84),
+ * solveOptions/{TemperatureThreshold, TemperatureAlpha, TemperatureBeta} and
+ * chemicalMaxStep (chemistrySource/src/chemistrySource.cpp:42-84).
+ */
+typedef struct hc_opts {
+    int32_t maxstep;             /* 10000 */
+    int32_t auto_update_jacobian;/* 0 */
+    int32_t step_to_update_jac;  /* 10 */
+    int32_t reactor;             /* 0 constant pressure (only form built) */
+    double atol;                 /* 1e-15 (reference default "tiny") */
+    double rtol;                 /* 1e-4 */
+    double safescale;            /* 0.8 */
+    double minscale;             /* 0.25 */
+    double maxscale;             /* 2.0 */
+    double alphainc;             /* 0.25 */
+    double atol_increment;       /* 1e-7 */
+    double rtol_increment;       /* 1e-3 */
+    double T_threshold;          /* 200 K */
+    double T_alpha;              /* 0.2 */
+    double T_beta;               /* 0.25 */
+    double dt_max;               /* chemicalMaxStep, 1e15 ("large") */
+    int64_t max_newton_total;    /* safety cap per cell per call, 0 = none */
+} hc_opts;
+
+/* per-call work counters (summed over cells) */
+typedef struct hc_counters {
+    int64_t n_jac;       /* Jacobian evaluations (each also yields f) */
+    int64_t n_rhs;       /* right-hand-side-only evaluations */
+    int64_t n_lu;        /* LU factorisations */
+    int64_t n_newton;    /* Newton iterations */
+    int64_t n_steps;     /* accepted steps */
+    int64_t n_attempts;  /* step attempts */
+} hc_counters;
+
+typedef struct hc_mech_s *hc_mech_t;
+
+int hc_abi_version(void);
+const char *hc_last_error(void);
+void hc_default_opts(hc_opts *opts);
+
+/* Upload a mechanism; selects the compiled kernel variant for nsp. */
+int hc_mech_create(const hc_mech_desc *desc, hc_mech_t *out);
+int hc_mech_destroy(hc_mech_t mech);
+int hc_mech_nsp(hc_mech_t mech);
+int hc_mech_nrc(hc_mech_t mech);
+
+/*
+ * Integrate ncells cells over dt[cell] * dt_factor with device pointers.
+ * Replaces chemistrySource::solve(const realArray &dt, real dtFactor) and
+ * chemistrySource::solveUpdate (chemistrySource/src/chemistrySource.cpp:1494-1609)
+ * for the ODESolver<chemistrySource> + ImplicitEuler configuration.
+ *   T[ncells]        in: temperature; out: T after the step
+ *   p[ncells]        pressure (constant during the step)
+ *   rho[ncells]      in: density; out: rho(p, T, Y) after the step
+ *   Y[nsp*ncells]    in: mass fractions; out: renormalised mass fractions
+ *   dt[ncells]       flow time step per cell
+ *   subdt[ncells]    in/out warm-start sub-step (the reference's dtInit);
+ *                    pass dt on the first flow step
+ *   Ri[nsp*ncells]   optional out (may be NULL): (c_new - c_old)/(dt*dt_factor)*W_i
+ *   status[ncells]   optional out: HC_CELL_* bits
+ *   counters         optional out (host struct; forces a stream sync)
+ */
+int hc_integrate(hc_mech_t mech, const hc_opts *opts, int64_t ncells, double *T, const double *p,
+                 double *rho, double *Y, const double *dt, double dt_factor, double *subdt,
+                 double *Ri, int32_t *status, hc_counters *counters, void *stream);
+
+/* Same with host buffers: H2D, integrate, D2H, synchronise. */
+int hc_integrate_host(hc_mech_t mech, const hc_opts *opts, int64_t ncells, double *T,
+                      const double *p, double *rho, double *Y, const double *dt, double dt_factor,
+                      double *subdt, double *Ri, int32_t *status, hc_counters *counters,
+                      void *stream);
+
+/*
+ * Right-hand side and analytic Jacobian of the constant-pressure reactor at
+ * given states (chemistrySource::DyDt / ::jacobian, chemistrySource.cpp:863,967).
+ *   c[nsp*n], T[n], p[n] -> dydt[(nsp+1)*n] (optional), J[(nsp+1)^2 * n] row-major
+ *   per state (optional).
+ */
+int hc_rhs_jacobian(hc_mech_t mech, int64_t n, const double *c, const double *T, const double *p,
+                    double *dydt, double *J, void *stream);
+
+/*
+ * Explicit source terms omega_i * W_i [kg/m^3/s] (chemistrySource::calculateSourceTerms,
+ * chemistrySource.cpp:1370-1406): T, p, rho, Y -> Ri[nsp*n].
+ */
+int hc_source_terms(hc_mech_t mech, int64_t n, const double *T, const double *p, const double *rho,
+                    const double *Y, double *Ri, void *stream);
+
+/*
+ * Mixture properties (thermoList / transportList, kinetic theory + Wilke):
+ * T, p, Y -> ha[nsp*n] (J/kg per species), cp[n] (J/kg/K), mu[n] (Pa s),
+ * kappa[n] (W/m/K), D[nsp*n] (m^2/s mixture-averaged). Any output may be NULL.
+ */
+int hc_properties(hc_mech_t mech, int64_t n, const double *T, const double *p, const double *Y,
+                  double *ha, double *cp, double *mu, double *kappa, double *D, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HURCHEM_B200_H */

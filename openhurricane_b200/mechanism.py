@@ -1,0 +1,376 @@
+"""Mechanism reader and compiler: Chemkin + NASA-7 + transport -> flat tables.
+
+This is the host-side half of the drop-in boundary. It reads the three text
+files the reference reads (chemistryRead/src/chemkinFileRead.cpp,
+JANAFThermoParsing.cpp, JANAFTransportParsing.cpp) and produces the flat,
+structure-of-arrays tables that the C ABI (`hc_mech_create`, declared in
+include/hurchem_b200.h) uploads to the GPU. Unit conversions and derived
+constants are computed with the same floating-point operations, in the same
+order, as the reference so that the tables hold identical bits:
+
+* R = kB * NA [J/mol/K], Ru = R * 1e3 [J/kmol/K]
+  (Hurricane/common/constants/physicalConstant.hpp:158,183);
+* W_i = sum of n_atoms * atomic weight in file order (species.cpp:92);
+  R_i = Ru / W_i;
+* NASA-7 coefficients are converted to the mass basis, a_k * R_i
+  (thermo/src/JANAF.cpp:44-58);
+* A is scaled by pow(1e-3, order - 1) with order = sum of forward orders, an
+  extra 1e-3 for '+M' third-body reactions and for the low-pressure limit of
+  fall-off reactions; E [cal/mol] becomes Ta = E / (R / 4.184)
+  (chemkinFileRead.cpp:1374-1455, :1654-1696);
+* the species of each side are held in a name-sorted map, repeated species
+  merged (chemkinFileRead.cpp:902-925), so the forward/backward coefficient
+  lists are in lexicographic name order;
+* third-body efficiencies default to 1.0 for every species
+  (chemkinFileRead.cpp:1050-1061, :1063-1085).
+
+Supported rate forms: Arrhenius, Arrhenius third-body (+M), unimolecular
+fall-off (+M) with Lindemann or Troe (3 or 4 parameters); reversible (=, <=>)
+and irreversible (=>) reactions.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import re
+from typing import Dict, List, Optional, Tuple
+
+import numpy as np
+
+# physical constants, evaluated exactly as the reference's constexprs
+KB = 1.380649e-23
+NA = 6.02214076e23
+R_J_MOL_K = KB * NA
+RU = R_J_MOL_K * 1e3
+PATM = 1.01325e5
+CAL_TH = 4.184
+
+# element table entries for the elements that may appear (standard atomic
+# weights; species/include/atomicWeights.hpp holds the same numbers)
+ATOMIC_WEIGHTS = {
+    "H": 1.00797, "D": 2.01410, "HE": 4.00260, "C": 12.01115, "N": 14.00670,
+    "O": 15.99940, "F": 18.99840, "NE": 20.18300, "S": 32.06400, "CL": 35.45300,
+    "AR": 39.94800,
+}
+
+MAX_SIDE = 4          # species per reaction side held in the flat tables
+
+# rate-law codes of the flat tables
+RATE_ARRHENIUS = 0
+RATE_THIRD_BODY = 1
+RATE_LINDEMANN = 2
+RATE_TROE3 = 3
+RATE_TROE4 = 4
+
+
+@dataclasses.dataclass
+class ParsedReaction:
+    fwd: List[Tuple[int, float]]      # (species index, stoich) name-sorted
+    bwd: List[Tuple[int, float]]
+    reversible: bool
+    A: float
+    b: float
+    E: float
+    kind: str                         # arrhenius | third_body | falloff
+    eff: Optional[np.ndarray] = None
+    low: Optional[Tuple[float, float, float]] = None
+    troe: Optional[List[float]] = None
+
+
+@dataclasses.dataclass
+class MechTables:
+    """Flat tables in SI units (kmol, m^3, s, K, J, kg)."""
+    names: List[str]
+    W: np.ndarray            # [nsp]
+    Ri: np.ndarray           # [nsp]
+    Trange: np.ndarray       # [nsp, 3] Tlow, Tcommon, Thigh
+    nasa: np.ndarray         # [nsp, 2, 7] mass basis: [low, high]
+    elem_names: List[str]
+    elem_matrix: np.ndarray  # [nelem, nsp] atoms per species
+    rate_type: np.ndarray    # [nrc] int32
+    reversible: np.ndarray   # [nrc] int32
+    arr: np.ndarray          # [nrc, 3] A, beta, Ta (high-pressure limit for fall-off)
+    arr0: np.ndarray         # [nrc, 3] low-pressure limit (fall-off only)
+    troe: np.ndarray         # [nrc, 4] alpha, T***, T*, T**
+    eff: np.ndarray          # [nrc, nsp] third-body efficiencies (1.0 unused rows)
+    nf: np.ndarray           # [nrc] int32
+    nb: np.ndarray           # [nrc] int32
+    fidx: np.ndarray         # [nrc, MAX_SIDE] int32
+    bidx: np.ndarray
+    fnu: np.ndarray          # [nrc, MAX_SIDE] stoichiometric coefficients
+    bnu: np.ndarray
+    ford: np.ndarray         # [nrc, MAX_SIDE] reaction orders
+    bord: np.ndarray
+    sum_stoi: np.ndarray     # [nrc] sum(bnu) - sum(fnu)
+    # transport (kinetic theory)
+    geom: np.ndarray         # [nsp] int32
+    eps_k: np.ndarray        # [nsp]
+    sigma: np.ndarray        # [nsp]
+    dipole: np.ndarray
+    polar: np.ndarray
+    zrot: np.ndarray
+
+    @property
+    def nsp(self) -> int:
+        return len(self.names)
+
+    @property
+    def nrc(self) -> int:
+        return int(self.rate_type.shape[0])
+
+
+def _strip_comments(text: str) -> str:
+    return "\n".join(line.split("!", 1)[0] for line in text.splitlines())
+
+
+def _section(text: str, start_re: str) -> str:
+    m = re.search(start_re + r"\s+([\s\S]*?)\s+END", text, re.IGNORECASE)
+    return m.group(1) if m else ""
+
+
+def _read_real(s: str) -> float:
+    s = s.strip().replace("D", "E").replace("d", "e")
+    return float(s)
+
+
+def _parse_side(txt: str, index: Dict[str, int]) -> List[Tuple[int, float]]:
+    counts: Dict[str, float] = {}
+    for term in txt.split("+"):
+        term = term.strip()
+        if not term:
+            continue
+        m = re.match(r"^((?:[0-9]*)\.*[0-9]*)\s*(\S+)$", term)
+        coef = float(m.group(1)) if m.group(1) else 1.0
+        name = m.group(2)
+        counts[name] = counts.get(name, 0.0) + coef
+    out = []
+    for name in sorted(counts):           # std::map order
+        if name not in index:
+            raise ValueError(f"unknown species {name!r}")
+        out.append((index[name], counts[name]))
+    return out
+
+
+def _split_side_terms(side: str) -> str:
+    # '+' signs that separate species (a leading '+' of a charge is not used here)
+    return side
+
+
+def parse_chemkin(che_text: str, species_names: Optional[List[str]] = None):
+    text = _strip_comments(che_text)
+    sp_txt = _section(text, r"SPEC(?:|IE|IES)")
+    names = species_names or sp_txt.split()
+    index = {n: i for i, n in enumerate(names)}
+    el_txt = _section(text, r"ELEM(?:|ENT|ENTS)")
+    elements = [e.upper() for e in el_txt.split()]
+    rx_txt = _section(text, r"REAC(?:|TION|TIONS)")
+    lines = [l for l in rx_txt.splitlines() if l.strip()]
+    line_re = re.compile(r"^(.*?)\s*(<=>|=>|=)\s*(.*?)\s+([-+]?[0-9.]+(?:[eEdD][-+]?[0-9]+)?)"
+                         r"\s+(\S+)\s+(\S+)\s*$")
+    reactions: List[ParsedReaction] = []
+    cur: Optional[ParsedReaction] = None
+    for line in lines:
+        m = line_re.match(line.strip())
+        if m and ("=" in m.group(2)):
+            lhs, arrow, rhs = m.group(1), m.group(2), m.group(3)
+            A, b, E = _read_real(m.group(4)), _read_real(m.group(5)), _read_real(m.group(6))
+            kind = "arrhenius"
+            pd = re.compile(r"\(\s*\+\s*(\S+?)\s*\)")
+            if pd.search(lhs) or pd.search(rhs):
+                third = pd.search(lhs).group(1)
+                if third.upper() != "M":
+                    raise NotImplementedError("species-specific (+X) fall-off")
+                lhs, rhs = pd.sub("", lhs), pd.sub("", rhs)
+                kind = "falloff"
+            tb = re.compile(r"\+\s*M(?![-a-zA-Z0-9])", re.IGNORECASE)
+            if tb.search(lhs) or tb.search(rhs):
+                lhs, rhs = tb.sub("", lhs), tb.sub("", rhs)
+                kind = "third_body"
+            cur = ParsedReaction(_parse_side(lhs, index), _parse_side(rhs, index),
+                                 arrow != "=>", A, b, E, kind)
+            if kind in ("third_body", "falloff"):
+                cur.eff = np.ones(len(names))
+            reactions.append(cur)
+            continue
+        # auxiliary line
+        s = line.strip()
+        up = s.upper()
+        if up.startswith("LOW"):
+            v = re.search(r"LOW\s*/\s*(.*?)\s*/", s, re.IGNORECASE).group(1).split()
+            cur.low = (_read_real(v[0]), _read_real(v[1]), _read_real(v[2]))
+        elif up.startswith("TROE"):
+            v = re.search(r"TROE\s*/\s*(.*?)\s*/", s, re.IGNORECASE).group(1).split()
+            cur.troe = [_read_real(x) for x in v]
+        elif up.startswith("DUP"):
+            continue
+        else:
+            for nm, val in re.findall(r"(\S+?)\s*/\s*([^/]+?)\s*/", s):
+                if nm not in index:
+                    raise ValueError(f"unknown efficiency species {nm!r}")
+                cur.eff[index[nm]] = _read_real(val)
+    return names, elements, reactions
+
+
+def parse_thermo(text: str, names: List[str]):
+    lines = [l.split("!", 1)[0] if not l.startswith("!") else "" for l in text.splitlines()]
+    lines = [l for l in lines if l.strip() != ""]
+    glob = None
+    for l in lines[:3]:
+        nums = l.split()
+        if len(nums) == 3:
+            try:
+                glob = [float(x) for x in nums]
+            except ValueError:
+                pass
+    found = {}
+    i = 0
+    while i + 3 < len(lines):
+        l1 = lines[i]
+        if len(l1) >= 80 and l1[79] == "1":
+            name = l1[0:18].split()[0]
+            if name in names and name not in found:
+                tlow = float(l1[45:55])
+                thigh = float(l1[55:65])
+                tc_txt = l1[65:73].strip()
+                tcommon = float(tc_txt) if tc_txt else glob[1]
+                elstr = l1[24:44]
+                els = []
+                for k in range(4):
+                    e = elstr[k * 5:k * 5 + 2].strip()
+                    c = elstr[k * 5 + 2:k * 5 + 5].strip()
+                    if c and int(c) != 0:
+                        els.append((e.upper(), int(c)))
+                l2, l3, l4 = lines[i + 1], lines[i + 2], lines[i + 3]
+                f = lambda l, k: float(l[k * 15:(k + 1) * 15])
+                high = [f(l2, 0), f(l2, 1), f(l2, 2), f(l2, 3), f(l2, 4), f(l3, 0), f(l3, 1)]
+                low = [f(l3, 2), f(l3, 3), f(l3, 4), f(l4, 0), f(l4, 1), f(l4, 2), f(l4, 3)]
+                found[name] = (tlow, tcommon, thigh, els, low, high)
+            i += 4
+        else:
+            i += 1
+    missing = [n for n in names if n not in found]
+    if missing:
+        raise ValueError(f"thermo data missing for {missing}")
+    return found
+
+
+def parse_transport(text: str, names: List[str]):
+    out = {}
+    for line in text.splitlines():
+        line = line.split("!", 1)[0].strip()
+        if not line:
+            continue
+        tok = line.split()
+        if tok[0] in names and tok[0] not in out:
+            vals = [float(x) for x in tok[1:7]] + [0.0] * (6 - len(tok[1:7]))
+            out[tok[0]] = (int(vals[0]), vals[1], vals[2], vals[3], vals[4], vals[5])
+    return out
+
+
+def compile_mechanism(che_path: str, thermo_path: str, transport_path: str) -> MechTables:
+    with open(che_path) as f:
+        che = f.read()
+    names, elements, reactions = parse_chemkin(che)
+    with open(thermo_path) as f:
+        thermo = parse_thermo(f.read(), names)
+    with open(transport_path) as f:
+        tran = parse_transport(f.read(), names)
+    nsp, nrc = len(names), len(reactions)
+
+    W = np.zeros(nsp)
+    Ri = np.zeros(nsp)
+    Tr = np.zeros((nsp, 3))
+    nasa = np.zeros((nsp, 2, 7))
+    el_names = list(elements)
+    E = np.zeros((len(el_names), nsp))
+    for i, n in enumerate(names):
+        tlow, tcommon, thigh, els, low, high = thermo[n]
+        w = 0.0
+        for e, c in els:
+            w += c * ATOMIC_WEIGHTS[e]
+            if e not in el_names:
+                el_names.append(e)
+                E = np.vstack([E, np.zeros((1, nsp))])
+            E[el_names.index(e), i] += c
+        W[i] = w
+        Ri[i] = RU / w
+        Tr[i] = (tlow, tcommon, thigh)
+        for k in range(7):
+            nasa[i, 0, k] = low[k] * Ri[i]
+            nasa[i, 1, k] = high[k] * Ri[i]
+
+    rate_type = np.zeros(nrc, np.int32)
+    rev = np.zeros(nrc, np.int32)
+    arr = np.zeros((nrc, 3))
+    arr0 = np.zeros((nrc, 3))
+    troe = np.zeros((nrc, 4))
+    eff = np.ones((nrc, nsp))
+    nf = np.zeros(nrc, np.int32)
+    nb = np.zeros(nrc, np.int32)
+    fidx = np.zeros((nrc, MAX_SIDE), np.int32)
+    bidx = np.zeros((nrc, MAX_SIDE), np.int32)
+    fnu = np.zeros((nrc, MAX_SIDE))
+    bnu = np.zeros((nrc, MAX_SIDE))
+    ford = np.zeros((nrc, MAX_SIDE))
+    bord = np.zeros((nrc, MAX_SIDE))
+    sum_stoi = np.zeros(nrc)
+    RRcal = R_J_MOL_K / CAL_TH
+    for r, rx in enumerate(reactions):
+        if len(rx.fwd) > MAX_SIDE or len(rx.bwd) > MAX_SIDE:
+            raise ValueError("too many species on one side")
+        order = 0.0
+        for (_, nu) in rx.fwd:
+            order += nu
+        Afac = math.pow(0.001, order - 1.0)
+        Efac = RRcal
+        if rx.kind == "arrhenius":
+            rate_type[r] = RATE_ARRHENIUS
+            arr[r] = (rx.A * Afac, rx.b, rx.E / Efac)
+        elif rx.kind == "third_body":
+            rate_type[r] = RATE_THIRD_BODY
+            arr[r] = (1e-3 * rx.A * Afac, rx.b, rx.E / Efac)
+            eff[r] = rx.eff
+        else:
+            if rx.low is None:
+                raise ValueError("fall-off reaction without LOW")
+            A0, b0, E0 = rx.low
+            arr0[r] = (A0 * (1e-3 * Afac), b0, E0 / Efac)
+            arr[r] = (rx.A * Afac, rx.b, rx.E / Efac)
+            eff[r] = rx.eff
+            if rx.troe is None:
+                rate_type[r] = RATE_LINDEMANN
+            elif len(rx.troe) == 3:
+                rate_type[r] = RATE_TROE3
+                troe[r, :3] = rx.troe
+            else:
+                rate_type[r] = RATE_TROE4
+                troe[r, :4] = rx.troe[:4]
+        rev[r] = 1 if rx.reversible else 0
+        nf[r], nb[r] = len(rx.fwd), len(rx.bwd)
+        s = 0.0
+        for k, (i, nu) in enumerate(rx.fwd):
+            fidx[r, k], fnu[r, k], ford[r, k] = i, nu, nu
+            s -= nu
+        for k, (i, nu) in enumerate(rx.bwd):
+            bidx[r, k], bnu[r, k], bord[r, k] = i, nu, nu
+            s += nu
+        sum_stoi[r] = s
+
+    geom = np.zeros(nsp, np.int32)
+    eps = np.ones(nsp)
+    sig = np.ones(nsp)
+    dip = np.zeros(nsp)
+    pol = np.zeros(nsp)
+    zr = np.zeros(nsp)
+    for i, n in enumerate(names):
+        if n in tran:
+            g, e_, s_, d_, p_, z_ = tran[n]
+            geom[i], eps[i], sig[i], dip[i], pol[i], zr[i] = g, e_, s_, d_, p_, z_
+    return MechTables(names, W, Ri, Tr, nasa, el_names, E, rate_type, rev, arr, arr0, troe,
+                      eff, nf, nb, fidx, bidx, fnu, bnu, ford, bord, sum_stoi,
+                      geom, eps, sig, dip, pol, zr)
+
+
+def element_matrix_mass(m: MechTables) -> np.ndarray:
+    """Atoms of each element per kg of each species: E[e, i] / W_i."""
+    return m.elem_matrix / m.W[None, :]
