@@ -135,6 +135,15 @@ int hc_abi_version(void);
 const char *hc_last_error(void);
 void hc_default_opts(hc_opts *opts);
 
+/*
+ * Kernel selection for hc_integrate*: kernel 0 = automatic (thread per cell
+ * when nsp + 1 <= 16, else a cell group of 32/64 lanes), 1 = thread per cell,
+ * 2 = cell group; block = threads per block of the thread-per-cell kernel
+ * (32, 64 or 128). Set by the autotuner (openhurricane_b200/autotune.py). No
+ * reference counterpart.
+ */
+int hc_set_tuning(hc_mech_t mech, int kernel, int block);
+
 /* Upload a mechanism; selects the compiled kernel variant for nsp. */
 int hc_mech_create(const hc_mech_desc *desc, hc_mech_t *out);
 int hc_mech_destroy(hc_mech_t mech);
@@ -161,7 +170,22 @@ int hc_integrate(hc_mech_t mech, const hc_opts *opts, int64_t ncells, double *T,
                  double *rho, double *Y, const double *dt, double dt_factor, double *subdt,
                  double *Ri, int32_t *status, hc_counters *counters, void *stream);
 
-/* Same with host buffers: H2D, integrate, D2H, synchronise. */
+/*
+ * hc_integrate with a work-queue order and a per-cell cost output: cells are
+ * taken from the device queue in the order order[0..ncells) (NULL: natural
+ * order), and cost[cell] receives the cell's Newton-iteration count (NULL:
+ * not written). Feeding a descending sort of the previous flow step's cost
+ * back as the next step's order starts the stiffest cells first
+ * (stiffness re-binning). No reference counterpart: the reference integrates
+ * cells in mesh order (chemistrySource.cpp:1511).
+ */
+int hc_integrate_ordered(hc_mech_t mech, const hc_opts *opts, int64_t ncells, double *T,
+                         const double *p, double *rho, double *Y, const double *dt,
+                         double dt_factor, double *subdt, double *Ri, int32_t *status,
+                         const int32_t *order, int64_t *cost, hc_counters *counters,
+                         void *stream);
+
+/* Same as hc_integrate with host buffers: H2D, integrate, D2H, synchronise. */
 int hc_integrate_host(hc_mech_t mech, const hc_opts *opts, int64_t ncells, double *T,
                       const double *p, double *rho, double *Y, const double *dt, double dt_factor,
                       double *subdt, double *Ri, int32_t *status, hc_counters *counters,
@@ -190,6 +214,13 @@ int hc_source_terms(hc_mech_t mech, int64_t n, const double *T, const double *p,
  */
 int hc_properties(hc_mech_t mech, int64_t n, const double *T, const double *p, const double *Y,
                   double *ha, double *cp, double *mu, double *kappa, double *D, void *stream);
+
+/*
+ * Measurement utility, no reference counterpart: runs an FP64 FMA-throughput
+ * probe on the current device (independent FMA chains on every SM) and
+ * returns the achieved TFLOP/s, the denominator of the integrator's roofline.
+ */
+int hc_probe_fp64_peak(int iters, double *tflops, void *stream);
 
 #ifdef __cplusplus
 }

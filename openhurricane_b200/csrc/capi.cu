@@ -1,0 +1,517 @@
+// C ABI of libhurchem_b200.so (declared in include/hurchem_b200.h).
+//
+// Host side of the drop-in boundary: uploads a flattened mechanism, picks
+// the compiled kernel variant for its size, and launches the integrators,
+// the right-hand-side/Jacobian evaluator, the source-term and the property
+// kernels. No entry point aborts; errors are returned as status codes with a
+// message in hc_last_error().
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "../../include/hurchem_b200.h"
+#include "variants.h"
+
+using namespace hc;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+
+#define HC_CUDA(call)                                                                     \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(HC_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+int upload(std::vector<void *> &owned, const T *src, size_t n, const T **dst) {
+    if (n == 0) {
+        *dst = nullptr;
+        return HC_OK;
+    }
+    void *d = nullptr;
+    HC_CUDA(cudaMalloc(&d, n * sizeof(T)));
+    owned.push_back(d);
+    HC_CUDA(cudaMemcpy(d, src, n * sizeof(T), cudaMemcpyHostToDevice));
+    *dst = static_cast<const T *>(d);
+    return HC_OK;
+}
+
+enum Variant { kV10 = 0, kV16, kV32, kV54, kV64 };
+
+}  // namespace
+
+struct hc_mech_s {
+    DevMech dm{};
+    int variant = -1;
+    std::vector<void *> owned;
+    // reusable device workspace for the host-buffer entry points
+    std::mutex mu;
+    void *ws = nullptr;
+    size_t ws_bytes = 0;
+    unsigned long long *queue = nullptr;   // [1 + 6] queue head, counters
+    int num_sms = 0;
+    // thread-per-cell integrator: per-cell buffer for the two previous step
+    // states (ImplicitEuler's yklast_), grown on demand
+    double *ylast = nullptr;
+    size_t ylast_cells = 0;
+    // kernel choice (hc_set_tuning): 0 automatic, 1 thread per cell, 2 cell group
+    int kernel = 0;
+    int block = 64;
+};
+
+namespace {
+
+int variant_for(int N) {
+    if (N == 10) return kV10;
+    if (N <= 16) return kV16;
+    if (N <= 32) return kV32;
+    if (N == 54) return kV54;
+    if (N <= 64) return kV64;
+    return -1;
+}
+
+#define HC_DISPATCH(m, FN, ...)                                        \
+    switch ((m)->variant) {                                            \
+    case kV10: return variant_##FN##_10(__VA_ARGS__);                  \
+    case kV16: return variant_##FN##_16(__VA_ARGS__);                  \
+    case kV32: return variant_##FN##_32(__VA_ARGS__);                  \
+    case kV54: return variant_##FN##_54(__VA_ARGS__);                  \
+    case kV64: return variant_##FN##_64(__VA_ARGS__);                  \
+    default: return fail(HC_E_UNSUPPORTED, "no kernel variant");       \
+    }
+
+IntegratorParams make_params(const hc_opts *o) {
+    IntegratorParams P;
+    P.maxstep = o->maxstep;
+    P.auto_update_jacobian = o->auto_update_jacobian;
+    P.step_to_update_jac = o->step_to_update_jac;
+    P.atol = o->atol;
+    P.rtol = o->rtol;
+    P.safescale = o->safescale;
+    P.minscale = o->minscale;
+    P.maxscale = o->maxscale;
+    P.alphainc = o->alphainc;
+    P.atol_inc = o->atol_increment;
+    P.rtol_inc = o->rtol_increment;
+    P.T_threshold = o->T_threshold;
+    P.T_alpha = o->T_alpha;
+    P.T_beta = o->T_beta;
+    P.dt_max = o->dt_max;
+    // evaluated with the host libm, as the reference does at run time (ImplicitEuler.cpp:287)
+    P.err_accept_limit = std::pow(o->maxscale / o->safescale, -1.0 / o->alphainc);
+    P.max_newton_total = o->max_newton_total;
+    return P;
+}
+
+int check_opts(const hc_opts *o) {
+    if (!o) return fail(HC_E_INVALID, "opts is null");
+    if (o->reactor != 0)
+        return fail(HC_E_UNSUPPORTED, "only the constant-pressure reactor is built");
+    if (o->maxstep <= 0 || o->step_to_update_jac <= 0)
+        return fail(HC_E_INVALID, "maxstep and step_to_update_jac must be positive");
+    if (!(o->alphainc > 0) || !(o->safescale > 0))
+        return fail(HC_E_INVALID, "alphainc and safescale must be positive");
+    return HC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hc_abi_version(void) { return HC_ABI_VERSION; }
+
+const char *hc_last_error(void) { return g_err.c_str(); }
+
+void hc_default_opts(hc_opts *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->maxstep = 10000;
+    o->auto_update_jacobian = 0;
+    o->step_to_update_jac = 10;
+    o->reactor = 0;
+    o->atol = 1e-15;
+    o->rtol = 1e-4;
+    o->safescale = 0.8;
+    o->minscale = 0.25;
+    o->maxscale = 2.0;
+    o->alphainc = 0.25;
+    o->atol_increment = 1e-7;
+    o->rtol_increment = 1e-3;
+    o->T_threshold = 200.0;
+    o->T_alpha = 0.2;
+    o->T_beta = 0.25;
+    o->dt_max = 1e15;
+    o->max_newton_total = 20000000;
+}
+
+int hc_mech_create(const hc_mech_desc *d, hc_mech_t *out) {
+    if (!d || !out) return fail(HC_E_INVALID, "null argument");
+    *out = nullptr;
+    const int nsp = d->nsp, nrc = d->nrc;
+    if (nsp < 1 || nrc < 0) return fail(HC_E_INVALID, "bad mechanism size");
+    const int variant = variant_for(nsp + 1);
+    if (variant < 0)
+        return fail(HC_E_UNSUPPORTED, "mechanisms with more than 63 species are not built");
+    if (!d->W || !d->Trange || !d->nasa || (nrc > 0 && (!d->rate_type || !d->reversible ||
+        !d->arr || !d->arr0 || !d->troe || !d->eff || !d->nf || !d->nb || !d->fidx ||
+        !d->bidx || !d->fnu || !d->bnu || !d->ford || !d->bord)))
+        return fail(HC_E_INVALID, "null table in mechanism");
+    for (int r = 0; r < nrc; ++r) {
+        if (d->nf[r] < 0 || d->nf[r] > HC_MAX_SIDE || d->nb[r] < 0 || d->nb[r] > HC_MAX_SIDE)
+            return fail(HC_E_INVALID, "reaction side larger than HC_MAX_SIDE");
+        if (d->rate_type[r] < 0 || d->rate_type[r] > HC_RATE_TROE4)
+            return fail(HC_E_INVALID, "unknown rate type");
+        for (int k = 0; k < d->nf[r]; ++k)
+            if (d->fidx[HC_MAX_SIDE * r + k] < 0 || d->fidx[HC_MAX_SIDE * r + k] >= nsp)
+                return fail(HC_E_INVALID, "species index out of range");
+        for (int k = 0; k < d->nb[r]; ++k)
+            if (d->bidx[HC_MAX_SIDE * r + k] < 0 || d->bidx[HC_MAX_SIDE * r + k] >= nsp)
+                return fail(HC_E_INVALID, "species index out of range");
+    }
+    // Reactions are regrouped by rate law (plain Arrhenius, third-body,
+    // fall-off), stable within a group, so that the lanes of a cell group
+    // evaluating one chunk of reactions mostly follow the same code path.
+    // Source terms are sums over reactions; only their summation order changes.
+    std::vector<int> perm(nrc);
+    for (int r = 0; r < nrc; ++r) perm[r] = r;
+    auto cls = [&](int r) { return d->rate_type[r] >= HC_RATE_LINDEMANN ? 2 : d->rate_type[r]; };
+    std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return cls(a) < cls(b); });
+    auto permute = [&](const auto *src, int width) {
+        using V = std::remove_const_t<std::remove_pointer_t<decltype(src)>>;
+        std::vector<V> outv((size_t)nrc * width);
+        for (int r = 0; r < nrc; ++r)
+            for (int k = 0; k < width; ++k)
+                outv[(size_t)r * width + k] = src[(size_t)perm[r] * width + k];
+        return outv;
+    };
+    const auto p_type = permute(d->rate_type, 1), p_rev = permute(d->reversible, 1);
+    const auto p_arr = permute(d->arr, 3), p_arr0 = permute(d->arr0, 3), p_troe = permute(d->troe, 4);
+    const auto p_eff = permute(d->eff, nsp);
+    const auto p_nf = permute(d->nf, 1), p_nb = permute(d->nb, 1);
+    const auto p_fidx = permute(d->fidx, HC_MAX_SIDE), p_bidx = permute(d->bidx, HC_MAX_SIDE);
+    const auto p_fnu = permute(d->fnu, HC_MAX_SIDE), p_bnu = permute(d->bnu, HC_MAX_SIDE);
+    const auto p_ford = permute(d->ford, HC_MAX_SIDE), p_bord = permute(d->bord, HC_MAX_SIDE);
+    // participation lists per species, in (regrouped) reaction order:
+    // coef = -nu' (reactant) / +nu'' (product)
+    std::vector<std::vector<std::pair<int, double>>> part(nsp);
+    std::vector<double> sum_stoi(nrc);
+    for (int r = 0; r < nrc; ++r) {
+        double s = 0.0;
+        for (int k = 0; k < p_nf[r]; ++k) {
+            part[p_fidx[HC_MAX_SIDE * r + k]].push_back({r, -p_fnu[HC_MAX_SIDE * r + k]});
+            s -= p_fnu[HC_MAX_SIDE * r + k];
+        }
+        for (int k = 0; k < p_nb[r]; ++k) {
+            part[p_bidx[HC_MAX_SIDE * r + k]].push_back({r, p_bnu[HC_MAX_SIDE * r + k]});
+            s += p_bnu[HC_MAX_SIDE * r + k];
+        }
+        sum_stoi[r] = s;
+    }
+    std::vector<int32_t> sp_ptr(nsp + 1, 0), sp_rxn;
+    std::vector<double> sp_coef;
+    for (int i = 0; i < nsp; ++i) {
+        sp_ptr[i] = (int32_t)sp_rxn.size();
+        for (auto &pr : part[i]) {
+            sp_rxn.push_back(pr.first);
+            sp_coef.push_back(pr.second);
+        }
+    }
+    sp_ptr[nsp] = (int32_t)sp_rxn.size();
+
+    hc_mech_s *m = new hc_mech_s();
+    m->variant = variant;
+    DevMech &dm = m->dm;
+    dm.nsp = nsp;
+    dm.nrc = nrc;
+    int rc = HC_OK;
+    auto up = [&](auto *src, size_t n, auto **dst) {
+        if (rc == HC_OK) rc = upload(m->owned, src, n, dst);
+    };
+    up(d->W, nsp, &dm.W);
+    up(d->Trange, 3 * (size_t)nsp, &dm.Trange);
+    up(d->nasa, 14 * (size_t)nsp, &dm.nasa);
+    up(p_type.data(), nrc, &dm.rate_type);
+    up(p_rev.data(), nrc, &dm.reversible);
+    up(p_arr.data(), 3 * (size_t)nrc, &dm.arr);
+    up(p_arr0.data(), 3 * (size_t)nrc, &dm.arr0);
+    up(p_troe.data(), 4 * (size_t)nrc, &dm.troe);
+    up(p_eff.data(), (size_t)nrc * nsp, &dm.eff);
+    up(p_nf.data(), nrc, &dm.nf);
+    up(p_nb.data(), nrc, &dm.nb);
+    up(p_fidx.data(), HC_MAX_SIDE * (size_t)nrc, &dm.fidx);
+    up(p_bidx.data(), HC_MAX_SIDE * (size_t)nrc, &dm.bidx);
+    up(p_ford.data(), HC_MAX_SIDE * (size_t)nrc, &dm.ford);
+    up(p_bord.data(), HC_MAX_SIDE * (size_t)nrc, &dm.bord);
+    up(p_fnu.data(), HC_MAX_SIDE * (size_t)nrc, &dm.fnu);
+    up(p_bnu.data(), HC_MAX_SIDE * (size_t)nrc, &dm.bnu);
+    up(sum_stoi.data(), nrc, &dm.sum_stoi);
+    up(sp_ptr.data(), nsp + 1, &dm.sp_ptr);
+    up(sp_rxn.data(), sp_rxn.size(), &dm.sp_rxn);
+    up(sp_coef.data(), sp_coef.size(), &dm.sp_coef);
+    if (d->geom) up(d->geom, nsp, &dm.geom);
+    if (d->eps_k) up(d->eps_k, nsp, &dm.eps_k);
+    if (d->sigma) up(d->sigma, nsp, &dm.sigma);
+    if (d->eps_k && d->sigma) {
+        // pair constants of kineticTheory::Di (kineticTheory.cpp:126-141) and of
+        // the Wilke factors (transportList.cpp:31-56), with the host libm
+        const size_t nn = (size_t)nsp * nsp;
+        std::vector<double> pD(nn), pP(nn), pR(nn), pPhi(nn), pW(nn);
+        const double c8 = 1.0 / std::sqrt(8.0);
+        for (int i = 0; i < nsp; ++i) {
+            const double invW = 1.0 / d->W[i];
+            for (int j = 0; j < nsp; ++j) {
+                const size_t k = (size_t)i * nsp + j;
+                const double sij = 0.5 * (d->sigma[i] + d->sigma[j]);
+                pD[k] = 1.858e-7 * std::sqrt(invW + 1.0 / d->W[j]) / (sij * sij) * 1.01325e5;
+                pR[k] = 1.0 / std::sqrt(d->eps_k[i] * d->eps_k[j]);
+                pP[k] = std::exp(-0.145 * std::log(pR[k]));
+                pPhi[k] = c8 / std::sqrt(1.0 + d->W[i] / d->W[j]);
+                pW[k] = std::sqrt(d->W[i] / d->W[j]);
+            }
+        }
+        up(pD.data(), nn, &dm.pair_D);
+        up(pP.data(), nn, &dm.pair_Dpow);
+        up(pR.data(), nn, &dm.pair_r);
+        up(pPhi.data(), nn, &dm.pair_phi);
+        up(pW.data(), nn, &dm.pair_w);
+    }
+    if (rc == HC_OK) {
+        void *q = nullptr;
+        cudaError_t e = cudaMalloc(&q, 8 * sizeof(unsigned long long));
+        if (e != cudaSuccess) {
+            rc = fail(HC_E_CUDA, cudaGetErrorString(e));
+        } else {
+            m->owned.push_back(q);
+            m->queue = static_cast<unsigned long long *>(q);
+        }
+    }
+    if (rc == HC_OK) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&m->num_sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    if (rc != HC_OK) {
+        for (void *p : m->owned) cudaFree(p);
+        delete m;
+        return rc;
+    }
+    *out = m;
+    return HC_OK;
+}
+
+int hc_set_tuning(hc_mech_t m, int kernel, int block) {
+    if (!m) return fail(HC_E_INVALID, "null mechanism");
+    if (kernel < 0 || kernel > 2) return fail(HC_E_INVALID, "kernel must be 0, 1 or 2");
+    if (block != 32 && block != 64 && block != 128)
+        return fail(HC_E_INVALID, "block must be 32, 64 or 128");
+    m->kernel = kernel;
+    m->block = block;
+    return HC_OK;
+}
+
+int hc_mech_destroy(hc_mech_t m) {
+    if (!m) return HC_OK;
+    for (void *p : m->owned) cudaFree(p);
+    if (m->ws) cudaFree(m->ws);
+    if (m->ylast) cudaFree(m->ylast);
+    delete m;
+    return HC_OK;
+}
+
+int hc_mech_nsp(hc_mech_t m) { return m ? m->dm.nsp : -1; }
+int hc_mech_nrc(hc_mech_t m) { return m ? m->dm.nrc : -1; }
+
+}  // extern "C"
+
+static int integrate_impl(hc_mech_t m, const hc_opts *opts, int64_t ncells, double *T,
+                          const double *p, double *rho, double *Y, const double *dt,
+                          double dt_factor, double *subdt, double *Ri, int32_t *status,
+                          const int32_t *order, int64_t *cost, cudaStream_t st) {
+    if (!m) return fail(HC_E_INVALID, "null mechanism");
+    int rc = check_opts(opts);
+    if (rc != HC_OK) return rc;
+    if (ncells < 0) return fail(HC_E_INVALID, "negative cell count");
+    HC_CUDA(cudaMemsetAsync(m->queue, 0, 7 * sizeof(unsigned long long), st));
+    if (ncells == 0) return HC_OK;
+    if (!T || !p || !rho || !Y || !dt || !subdt) return fail(HC_E_INVALID, "null field");
+    if (!(dt_factor > 0)) return fail(HC_E_INVALID, "dt_factor must be positive");
+    const IntegratorParams P = make_params(opts);
+    CellIO io;
+    io.ncells = ncells;
+    io.T = T;
+    io.p = p;
+    io.rho = rho;
+    io.Y = Y;
+    io.dt = dt;
+    io.dt_factor = dt_factor;
+    io.subdt = subdt;
+    io.Ri = Ri;
+    io.status = status;
+    io.order = order;
+    io.cost = cost;
+    io.queue_head = m->queue;
+    io.counters = m->queue + 1;
+    const int N = m->dm.nsp + 1;
+    const bool t1_ok = N <= 16 && !opts->auto_update_jacobian;
+    if (m->kernel == 1 && !t1_ok)
+        return fail(HC_E_UNSUPPORTED,
+                    "thread-per-cell kernel needs nsp <= 15 and autoUpdateJacobian off");
+    const bool use_t1 = t1_ok && (m->kernel == 0 || m->kernel == 1);
+    if (use_t1) {
+        if (m->ylast_cells < (size_t)ncells) {
+            // grows only: a first call with a new, larger size synchronises the
+            // stream and must therefore come before any stream capture
+            HC_CUDA(cudaStreamSynchronize(st));
+            if (m->ylast) HC_CUDA(cudaFree(m->ylast));
+            m->ylast = nullptr;
+            m->ylast_cells = 0;
+            HC_CUDA(cudaMalloc(&m->ylast, sizeof(double) * 2 * 16 * (size_t)ncells));
+            m->ylast_cells = (size_t)ncells;
+        }
+        return variant_integrate_t1(N, m->dm, m->num_sms, P, io, m->ylast, m->block, st, g_err);
+    }
+    HC_DISPATCH(m, integrate, m->dm, m->num_sms, P, io, st, g_err);
+}
+
+static int read_counters(hc_mech_t m, hc_counters *c, cudaStream_t st) {
+    if (!c) return HC_OK;
+    unsigned long long h[7];
+    HC_CUDA(cudaMemcpyAsync(h, m->queue, sizeof(h), cudaMemcpyDeviceToHost, st));
+    HC_CUDA(cudaStreamSynchronize(st));
+    c->n_jac = (int64_t)h[1];
+    c->n_rhs = (int64_t)h[2];
+    c->n_lu = (int64_t)h[3];
+    c->n_newton = (int64_t)h[4];
+    c->n_steps = (int64_t)h[5];
+    c->n_attempts = (int64_t)h[6];
+    return HC_OK;
+}
+
+static int count_bad_status(const int32_t *status_host, int64_t n) {
+    int bad = 0;
+    for (int64_t i = 0; i < n; ++i)
+        if (status_host[i] & (HC_CELL_UNDERFLOW | HC_CELL_ITER_LIMIT)) ++bad;
+    return bad;
+}
+
+extern "C" {
+
+int hc_integrate(hc_mech_t m, const hc_opts *opts, int64_t ncells, double *T, const double *p,
+                 double *rho, double *Y, const double *dt, double dt_factor, double *subdt,
+                 double *Ri, int32_t *status, hc_counters *counters, void *stream) {
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int rc = integrate_impl(m, opts, ncells, T, p, rho, Y, dt, dt_factor, subdt, Ri, status,
+                            nullptr, nullptr, st);
+    if (rc != HC_OK) return rc;
+    return read_counters(m, counters, st);
+}
+
+int hc_integrate_ordered(hc_mech_t m, const hc_opts *opts, int64_t ncells, double *T,
+                         const double *p, double *rho, double *Y, const double *dt,
+                         double dt_factor, double *subdt, double *Ri, int32_t *status,
+                         const int32_t *order, int64_t *cost, hc_counters *counters,
+                         void *stream) {
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int rc = integrate_impl(m, opts, ncells, T, p, rho, Y, dt, dt_factor, subdt, Ri, status,
+                            order, cost, st);
+    if (rc != HC_OK) return rc;
+    return read_counters(m, counters, st);
+}
+
+int hc_integrate_host(hc_mech_t m, const hc_opts *opts, int64_t ncells, double *T,
+                      const double *p, double *rho, double *Y, const double *dt,
+                      double dt_factor, double *subdt, double *Ri, int32_t *status,
+                      hc_counters *counters, void *stream) {
+    if (!m) return fail(HC_E_INVALID, "null mechanism");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (ncells <= 0)
+        return integrate_impl(m, opts, ncells, T, p, rho, Y, dt, dt_factor, subdt, Ri, status,
+                              nullptr, nullptr, st);
+    std::lock_guard<std::mutex> lk(m->mu);
+    const int nsp = m->dm.nsp;
+    const size_t n = (size_t)ncells;
+    const size_t bytes = sizeof(double) * (n * (5 + 2 * (size_t)nsp)) + sizeof(int32_t) * n + 256;
+    if (m->ws_bytes < bytes) {
+        HC_CUDA(cudaStreamSynchronize(st));
+        if (m->ws) cudaFree(m->ws);
+        m->ws = nullptr;
+        m->ws_bytes = 0;
+        HC_CUDA(cudaMalloc(&m->ws, bytes));
+        m->ws_bytes = bytes;
+    }
+    double *dT = static_cast<double *>(m->ws);
+    double *dp = dT + n, *drho = dp + n, *ddt = drho + n, *dsub = ddt + n;
+    double *dY = dsub + n, *dRi = dY + n * nsp;
+    int32_t *dst = reinterpret_cast<int32_t *>(dRi + n * nsp);
+    HC_CUDA(cudaMemcpyAsync(dT, T, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    HC_CUDA(cudaMemcpyAsync(dp, p, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    HC_CUDA(cudaMemcpyAsync(drho, rho, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    HC_CUDA(cudaMemcpyAsync(ddt, dt, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    HC_CUDA(cudaMemcpyAsync(dsub, subdt, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    HC_CUDA(cudaMemcpyAsync(dY, Y, sizeof(double) * n * nsp, cudaMemcpyHostToDevice, st));
+    int rc = integrate_impl(m, opts, ncells, dT, dp, drho, dY, ddt, dt_factor, dsub,
+                            Ri ? dRi : nullptr, dst, nullptr, nullptr, st);
+    if (rc != HC_OK) return rc;
+    HC_CUDA(cudaMemcpyAsync(T, dT, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    HC_CUDA(cudaMemcpyAsync(rho, drho, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    HC_CUDA(cudaMemcpyAsync(subdt, dsub, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    HC_CUDA(cudaMemcpyAsync(Y, dY, sizeof(double) * n * nsp, cudaMemcpyDeviceToHost, st));
+    if (Ri) HC_CUDA(cudaMemcpyAsync(Ri, dRi, sizeof(double) * n * nsp, cudaMemcpyDeviceToHost, st));
+    std::vector<int32_t> stat_h;
+    int32_t *stat_out = status;
+    if (!stat_out) {
+        stat_h.resize(n);
+        stat_out = stat_h.data();
+    }
+    HC_CUDA(cudaMemcpyAsync(stat_out, dst, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
+    rc = read_counters(m, counters, st);
+    if (rc != HC_OK) return rc;
+    HC_CUDA(cudaStreamSynchronize(st));
+    return count_bad_status(stat_out, ncells);
+}
+
+int hc_rhs_jacobian(hc_mech_t m, int64_t n, const double *c, const double *T, const double *p,
+                    double *dydt, double *J, void *stream) {
+    if (!m) return fail(HC_E_INVALID, "null mechanism");
+    if (n <= 0) return HC_OK;
+    if (!c || !T || !p) return fail(HC_E_INVALID, "null field");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    HC_DISPATCH(m, rhsjac, m->dm, n, c, T, p, dydt, J, st, g_err);
+}
+
+int hc_source_terms(hc_mech_t m, int64_t n, const double *T, const double *p, const double *rho,
+                    const double *Y, double *Ri, void *stream) {
+    if (!m) return fail(HC_E_INVALID, "null mechanism");
+    if (n <= 0) return HC_OK;
+    if (!T || !p || !rho || !Y || !Ri) return fail(HC_E_INVALID, "null field");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    HC_DISPATCH(m, source, m->dm, n, T, p, rho, Y, Ri, st, g_err);
+}
+
+int hc_properties(hc_mech_t m, int64_t n, const double *T, const double *p, const double *Y,
+                  double *ha, double *cp, double *mu, double *kappa, double *D, void *stream) {
+    if (!m) return fail(HC_E_INVALID, "null mechanism");
+    if (n <= 0) return HC_OK;
+    if (!T || !p || !Y) return fail(HC_E_INVALID, "null field");
+    if (!m->dm.geom || !m->dm.eps_k || !m->dm.sigma)
+        return fail(HC_E_INVALID, "mechanism has no transport data");
+    return launch_properties(m->dm, n, T, p, Y, ha, cp, mu, kappa, D,
+                             static_cast<cudaStream_t>(stream), g_err);
+}
+
+}  // extern "C"

@@ -1,0 +1,5 @@
+// Cell-group kernel variant for mechanisms whose N = nsp + 1 equations fit 32 (cell group of 32 lanes).
+#include "launch.cuh"
+#include "variants.h"
+
+HC_DEFINE_VARIANT(32, 32, 32)

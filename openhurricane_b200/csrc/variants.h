@@ -1,0 +1,38 @@
+// Per-size kernel variants of the cell-group integrator, right-hand-side /
+// Jacobian and source-term kernels (one translation unit each, see
+// variant_*.cu), the thread-per-cell integrator (variant_t1.cu) and the
+// property kernel (props.cu). Each entry returns an HC_* status and writes a
+// message to err on failure.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "integrator.cuh"
+
+#define HC_DECLARE_VARIANT(S)                                                                   \
+    int variant_integrate_##S(const hc::DevMech &m, int num_sms, const hc::IntegratorParams &P, \
+                              const hc::CellIO &io, cudaStream_t st, std::string &err);          \
+    int variant_rhsjac_##S(const hc::DevMech &m, int64_t n, const double *c, const double *T,   \
+                           const double *p, double *dydt, double *J, cudaStream_t st,           \
+                           std::string &err);                                                   \
+    int variant_source_##S(const hc::DevMech &m, int64_t n, const double *T, const double *p,   \
+                           const double *rho, const double *Y, double *Ri, cudaStream_t st,     \
+                           std::string &err);
+
+HC_DECLARE_VARIANT(10)
+HC_DECLARE_VARIANT(16)
+HC_DECLARE_VARIANT(32)
+HC_DECLARE_VARIANT(54)
+HC_DECLARE_VARIANT(64)
+
+int variant_integrate_t1(int N, const hc::DevMech &m, int num_sms, const hc::IntegratorParams &P,
+                         const hc::CellIO &io, double *ylast, int block, cudaStream_t st,
+                         std::string &err);
+
+namespace hc {
+int launch_properties(const DevMech &m, int64_t n, const double *T, const double *p,
+                      const double *Y, double *ha, double *cp, double *mu, double *kappa,
+                      double *D, cudaStream_t st, std::string &err);
+}

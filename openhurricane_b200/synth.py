@@ -205,9 +205,9 @@ def make_mechanism(nsp: int, nrc: int, n_third_body: int, n_troe: int,
         if elemental:
             h298 = 0.0
         elif natoms == 1:
-            h298 = rng.uniform(20000.0, 40000.0)      # atoms: endothermic
+            h298 = rng.uniform(12000.0, 25000.0)      # atoms: h/R in K (100-210 kJ/mol)
         else:
-            h298 = rng.uniform(-30000.0, 20000.0)     # h/R in K (~ +-250 kJ/mol)
+            h298 = rng.uniform(-8000.0, 4000.0)       # h/R in K (-67..+33 kJ/mol)
         s298 = rng.uniform(13.0, 18.0) + 2.5 * natoms
         low, high = _fit_nasa7(rng, natoms, linear, h298, s298)
         geom = 0 if natoms == 1 else (1 if linear else 2)

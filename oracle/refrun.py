@@ -32,18 +32,21 @@ def available() -> bool:
 def write_case(path: str, che: str, thermo: str, tran: str, opts: Optional[Dict] = None) -> None:
     """Case file for the driver: the mixture files and the chemistry-source
     solver options, in the reference's XML controller format (merged over the
-    built-in chemSolvers configuration by the driver)."""
+    built-in chemSolvers configuration by the driver). The property mode needs
+    a viscous flow model (flowModel="laminarFlow"): with the inviscid EulerFlow
+    the reference does not read transport data."""
     o = dict(ODEsSolver="ImplicitEuler", maxstep=10000, atol=1e-11, rtol=1e-4,
              safescale=0.8, minscale=0.25, maxScale=2.0, alphainc=0.25,
              autoUpdateJacobian="off", stepToUpdateJac=10, ATolIncrement=1e-7,
              RTolIncrement=1e-3, TemperatureThreshold=200.0, TemperatureAlpha=0.2,
-             TemperatureBeta=0.25, chemicalMaxStep=1e10, reactor="constPressure")
+             TemperatureBeta=0.25, chemicalMaxStep=1e10, reactor="constPressure",
+             flowModel="EulerFlow")
     if opts:
         o.update(opts)
     xml = f"""<?xml version="1.0" encoding="UTF-8" standalone="no"?>
 <Config>
   <flow>
-    <flowModel>EulerFlow</flowModel>
+    <flowModel>{o['flowModel']}</flowModel>
     <mixture>
       <equationOfState>perfectGas</equationOfState>
       <chemical>reaction</chemical>

@@ -1,0 +1,101 @@
+"""Generate the golden fixtures of tests/golden/ with the REFERENCE itself.
+
+Runs OpenHurricane's own CPU chemistry path (compiled from the reference
+sources by oracle/Makefile.ref into oracle/_ref/hurchem_ref) on seeded inputs
+and stores inputs and outputs:
+
+  small_ref.npz : 9-species / 21-reaction mechanism, 48 cells drawn like the
+                  small workload (T 1000-2500 K, p 1-5 atm, Y ~ Dirichlet(0.5)),
+                  dt = 1e-6 s, reference default solver options; integrated
+                  T, Y, rho, concentrations and warm-start sub-steps; plus KAT
+                  states: DyDt, analytic Jacobian, species thermo, kf/Kc/kr;
+                  plus mixture properties (h_i, cp, mu, kappa, D_i) of 32 cells.
+  large_ref.npz : 53-species / 325-reaction mechanism, 2 cells drawn like the
+                  large workload (T 800-2800 K, p 0.5-10 atm, Dirichlet(0.3)),
+                  dt = 1e-7 s; plus KAT states and properties of 16 cells.
+
+The mechanism files are regenerated from their seeds by
+openhurricane_b200.synth at test time; a SHA-256 of the generated text files
+is stored so that a change of the generator is detected.
+
+    python tests/golden/make_golden.py   (needs oracle/_ref/hurchem_ref)
+"""
+import hashlib
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from openhurricane_b200 import synth  # noqa: E402
+from oracle import refrun  # noqa: E402
+
+
+def files_sha(paths):
+    h = hashlib.sha256()
+    for p in paths:
+        with open(p, "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()
+
+
+def kat_states(nsp, n, seed):
+    rng = np.random.default_rng(seed)
+    T = rng.uniform(800, 3000, n)
+    p = rng.uniform(1, 5, n) * 101325.0
+    c = rng.dirichlet(np.full(nsp, 0.5), n).T.copy() * rng.uniform(0.001, 0.1, n)
+    c[0, 0] = 0.0                  # an absent species
+    c[1, min(1, n - 1)] = -1e-12   # a slightly negative one (clamped by the reference)
+    return T, p, np.ascontiguousarray(c)
+
+
+def make(name, mech, cells, dt, nkat, prop_cells, out):
+    work = tempfile.mkdtemp(prefix="golden_")
+    files = synth.write_chemkin(mech, work)
+    case = os.path.join(work, "case.cont")
+    refrun.write_case(case, *files, {"atol": 1e-15})
+    W = mech.weights()
+    rho = synth.mixture_density(W, cells)
+    res = refrun.integrate(case, cells.T, cells.p, rho, dt, dt, cells.Y,
+                           procs=os.cpu_count() or 1, workdir=work)
+    T, p, c = kat_states(len(mech.species), nkat, seed=4242)
+    k = refrun.kat(case, p, T, c, workdir=work)
+    pcase = os.path.join(work, "case_props.cont")
+    refrun.write_case(pcase, *files, {"flowModel": "laminarFlow"})
+    pr = refrun.props(pcase, prop_cells.T, prop_cells.p, synth.mixture_density(W, prop_cells),
+                      prop_cells.Y, workdir=work)
+    np.savez_compressed(
+        out, sha=files_sha(files), seed=mech.seed, dt=dt,
+        in_T=cells.T, in_p=cells.p, in_rho=rho, in_Y=cells.Y,
+        out_T=res["T"], out_Y=res["Y"], out_rho=res["rho"], out_c=res["c"],
+        out_subdt=res["subdt"], out_status=res["status"],
+        kat_T=T, kat_p=p, kat_c=c, kat_dydt=k["dydt"], kat_J=k["J"],
+        kat_thermo=np.stack([k[n] for n in ("cp0", "ha0", "s0", "g0", "G0", "DG0DT", "Dcp_pDT")],
+                            axis=-1),
+        kat_rates=np.stack([k["kf"], k["Kc"], k["kr"]], axis=-1),
+        prop_T=prop_cells.T, prop_p=prop_cells.p, prop_Y=prop_cells.Y,
+        prop_ha=pr["ha"], prop_cp=pr["cp"], prop_mu=pr["mu"], prop_kappa=pr["kappa"],
+        prop_D=pr["D"])
+    print(name, "written", out, "reference seconds", res["seconds"])
+
+
+def main():
+    if not refrun.available():
+        raise SystemExit("oracle/_ref/hurchem_ref is missing: make -f oracle/Makefile.ref")
+    small = synth.small_mechanism()
+    make("small", small, synth.dirichlet_cells(9, 48, seed=101), 1e-6, 8,
+         synth.dirichlet_cells(9, 32, seed=105), os.path.join(HERE, "small_ref.npz"))
+    large = synth.large_mechanism()
+    make("large", large, synth.dirichlet_cells(53, 2, seed=103, T_range=(800, 2800),
+                                               p_atm_range=(0.5, 10), alpha=0.3),
+         1e-7, 3, synth.dirichlet_cells(53, 16, seed=107, T_range=(800, 2800),
+                                         p_atm_range=(0.5, 10), alpha=0.3),
+         os.path.join(HERE, "large_ref.npz"))
+
+
+if __name__ == "__main__":
+    main()

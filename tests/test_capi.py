@@ -1,0 +1,55 @@
+"""The C-ABI library loads without a GPU and exports every declared symbol."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = []
+    for fn in os.listdir(os.path.join(ROOT, "include")):
+        if not fn.endswith(".h"):
+            continue
+        txt = open(os.path.join(ROOT, "include", fn)).read()
+        txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+        names += re.findall(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b(hc_\w+)\s*\(", txt, flags=re.M)
+    return sorted(set(names))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    for must in ("hc_mech_create", "hc_integrate", "hc_integrate_host", "hc_source_terms",
+                 "hc_properties", "hc_rhs_jacobian", "hc_last_error"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    from openhurricane_b200 import _capi
+    if not os.path.isfile(_capi.LIB_PATH):
+        pytest.fail("libhurchem_b200.so not built: python -m openhurricane_b200.build")
+    lib = _capi.load()
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+        assert name in _capi.SIGNATURES, name
+    assert lib.hc_abi_version() == 1
+
+
+def test_default_opts_match_reference_defaults():
+    from openhurricane_b200 import _capi
+    o = _capi.default_opts()
+    assert (o.maxstep, o.rtol, o.atol, o.safescale, o.minscale, o.maxscale, o.alphainc) == \
+        (10000, 1e-4, 1e-15, 0.8, 0.25, 2.0, 0.25)
+    assert (o.atol_increment, o.rtol_increment, o.step_to_update_jac) == (1e-7, 1e-3, 10)
+    assert (o.T_threshold, o.T_alpha, o.T_beta) == (200.0, 0.2, 0.25)
+
+
+def test_invalid_arguments_fail_loudly_without_gpu():
+    from openhurricane_b200 import _capi
+    lib = _capi.load()
+    h = C.c_void_p()
+    assert lib.hc_mech_create(None, C.byref(h)) == -1
+    assert b"null" in lib.hc_last_error()
+    assert lib.hc_set_tuning(None, 0, 64) == -1

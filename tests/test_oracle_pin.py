@@ -1,0 +1,93 @@
+"""The oracle (oracle/chem_oracle.c, oracle/props_oracle.py) is pinned to the
+reference.
+
+1. Against the committed golden fixtures, which the reference itself
+   produced (tests/golden/make_golden.py): bit-for-bit equality of the
+   integrated states and of the kernel-level known answers (DyDt, analytic
+   Jacobian, NASA-7 thermo, kf/Kc/kr); properties within 1e-15 relative.
+2. Against the reference compiled from source here (oracle/_ref/hurchem_ref),
+   when that binary is present, on freshly drawn cells.
+"""
+import hashlib
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _sha(paths):
+    h = hashlib.sha256()
+    for p in paths:
+        with open(p, "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()
+
+
+def _load(name):
+    return np.load(os.path.join(HERE, "golden", f"{name}_ref.npz"))
+
+
+@pytest.mark.parametrize("name", ["small", "large"])
+def test_generator_reproduces_golden_mechanism(name, small, large):
+    mk = small if name == "small" else large
+    assert _sha(mk["files"]) == str(_load(name)["sha"])
+
+
+@pytest.mark.parametrize("name", ["small", "large"])
+def test_oracle_integration_bit_exact_vs_reference_golden(name, small, large):
+    from oracle import port
+    mk = small if name == "small" else large
+    g = _load(name)
+    md = port.MechDesc(mk["tables"])
+    o = port.integrate(md, g["in_T"], g["in_p"], g["in_rho"], g["in_Y"], float(g["dt"]),
+                       opts=port.default_opts(atol=1e-15))
+    for k in ("T", "Y", "rho", "c", "subdt"):
+        assert np.array_equal(o[k], g["out_" + k]), k
+
+
+@pytest.mark.parametrize("name", ["small", "large"])
+def test_oracle_kernels_bit_exact_vs_reference_golden(name, small, large):
+    from oracle import port
+    mk = small if name == "small" else large
+    g = _load(name)
+    md = port.MechDesc(mk["tables"])
+    dydt, J = port.rhs_jac(md, g["kat_c"], g["kat_T"])
+    assert np.array_equal(dydt, g["kat_dydt"])
+    assert np.array_equal(J, g["kat_J"])
+    for s in range(g["kat_T"].shape[0]):
+        assert np.array_equal(port.thermo(md, g["kat_T"][s]), g["kat_thermo"][s])
+        assert np.array_equal(port.rates(md, g["kat_T"][s], g["kat_c"][:, s]), g["kat_rates"][s])
+
+
+@pytest.mark.parametrize("name", ["small", "large"])
+def test_property_oracle_vs_reference_golden(name, small, large):
+    from oracle import props_oracle
+    mk = small if name == "small" else large
+    g = _load(name)
+    o = props_oracle.properties(mk["tables"], g["prop_T"], g["prop_p"], g["prop_Y"])
+    for k in ("ha", "cp", "mu", "kappa", "D"):
+        ref = g["prop_" + k]
+        assert np.max(np.abs(o[k] - ref) / np.maximum(np.abs(ref), 1e-300)) < 1e-15, k
+
+
+def test_oracle_bit_exact_vs_reference_binary(small):
+    from oracle import refrun, port
+    from openhurricane_b200 import synth
+    if not refrun.available():
+        pytest.skip("reference binary not built (make -f oracle/Makefile.ref)")
+    t = small["tables"]
+    work = tempfile.mkdtemp()
+    case = os.path.join(work, "case.cont")
+    refrun.write_case(case, *small["files"], {"atol": 1e-15, "rtol": 1e-5})
+    cells = synth.dirichlet_cells(t.nsp, 12, seed=2024)
+    cells.T[0] = 150.0      # below the 200 K threshold: skipped, dtInit = dt
+    rho = synth.mixture_density(t.W, cells)
+    r = refrun.integrate(case, cells.T, cells.p, rho, 1e-6, 5e-7, cells.Y, procs=4, workdir=work)
+    o = port.integrate(port.MechDesc(t), cells.T, cells.p, rho, cells.Y, 1e-6, subdt=5e-7,
+                       opts=port.default_opts(atol=1e-15, rtol=1e-5))
+    for k in ("T", "Y", "rho", "c", "subdt"):
+        assert np.array_equal(o[k], r[k]), k
+    assert o["status"][0] == 1 and r["status"][0] == 1
