@@ -1,0 +1,438 @@
+"""Chemistry source-term benchmark: cells/s per flow step on one B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload batched|small|large] [--cells n]
+
+A step is one flow step of the chemistry source: every cell of the workload
+is integrated over dt by the FP64 implicit-Euler integrator (one persistent
+work-queue launch, cells ordered stiffest-first by the previous step's
+Newton counts). Each step starts from the same seeded inputs, restored from a
+pristine device copy and followed by an L2 flush (a 256 MiB write) outside
+the per-step CUDA-event window.
+
+Workloads (seeded synthetic; no public dataset exists for this path):
+  batched  9 species / 21 reactions, 1,048,576 cells, 20 % near ignition and
+           80 % near equilibrium, dt = 1e-5 s          (default)
+  small    same mechanism, 4096 cells, Dirichlet states, dt = 1e-6 s
+  large    53 species / 325 reactions, 262,144 cells, dt = 1e-6 s
+
+Keys beyond the value: `e2e` is the same metric through hc_integrate_host
+with pinned host buffers (copies in the timed region); `roofline` is the
+integrator kernel's algorithmic FP64 FLOP rate (flop model of
+openhurricane_b200/workloads.py times the Newton/Jacobian/LU counters) over
+the FP64 FMA peak measured live by hc_probe_fp64_peak on this GPU;
+`cpu_baseline` is the reference's own CPU integrator (oracle/_ref/hurchem_ref,
+built from the reference sources) on a bounded sample of the same cells, one
+process per host core.
+
+--impl reference times that reference CPU path alone on the same workload,
+config, metric and unit. With N > 1 ranks (torchrun), every rank integrates
+its own replica of the workload (the path does not shard: replicas only);
+the time is the max over ranks and the value counts all ranks' cells.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "chem cells/s per flow step, plain FP64 vs gated surrogate @ max|ΔT|<5K, 1 B200"
+UNIT = "cells/s"
+WORKLOAD_CELLS = {"batched": 1048576, "small": 4096, "large": 262144}
+L2_FLUSH_BYTES = 256 << 20
+
+
+# ----------------------------------------------------------------------------- helpers
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for k, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(k)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- workloads
+def build_workload(name: str, ncells: int, seed_offset: int, relax_mech=None):
+    from openhurricane_b200 import workloads
+    if name == "small":
+        return workloads.make_small(ncells, seed=1001 + seed_offset)
+    if name == "large":
+        return workloads.make_large(ncells, seed=3003 + seed_offset)
+    if name == "batched":
+        def relax(T, p, rho, Y, t_relax):
+            from openhurricane_b200.chemistry import Mechanism, integrate_host
+            return_mech = relax_mech["mech"]
+            r = integrate_host(return_mech, T.copy(), p.copy(), rho.copy(), Y.copy(),
+                               np.full(T.shape[0], t_relax), **workloads.SOLVER_OPTS)
+            return r["T"], r["rho"], r["Y"]
+        return workloads.make_batched(ncells, seed=2002 + seed_offset, relax=relax)
+    raise ValueError(f"unknown workload {name}")
+
+
+def workload_config(wl, name: str) -> dict:
+    return {"workload": f"{name}: {wl.tables.nsp} species / {wl.tables.nrc} reactions, "
+                        f"{wl.n} cells, dt={wl.dt:g} s" + (f" ({wl.note})" if wl.note else ""),
+            "species": int(wl.tables.nsp), "reactions": int(wl.tables.nrc), "cells": wl.n,
+            "dt_s": wl.dt, "solver": "ImplicitEuler atol 1e-11 rtol 1e-4 maxstep 10000",
+            "l2": "256 MiB L2 flush between timed steps"}
+
+
+# ----------------------------------------------------------------------------- reference CPU
+def reference_cpu(wl, target_seconds: float, cores: int, sample_offset: int = 0):
+    """Time the reference's CPU integrator on a strided sample of the
+    workload's cells. Returns (cells/s, sample cells, seconds, kind, note)."""
+    from oracle import refrun
+    from openhurricane_b200 import workloads
+    if not refrun.available():
+        return None
+    work = tempfile.mkdtemp(prefix="hc_refbench_")
+    case = os.path.join(work, "case.cont")
+    refrun.write_case(case, *wl.files, dict(workloads.SOLVER_OPTS))
+    n = wl.n
+    # calibrate: one process on a handful of cells
+    cal = np.arange(sample_offset % 16, n, max(1, n // 64))[:64]
+    r = refrun.integrate(case, wl.T[cal], wl.p[cal], wl.rho[cal], wl.dt, wl.dt,
+                         wl.Y[:, cal], procs=1, workdir=work)
+    per_cell = max(r["seconds"], 1e-6) / cal.size
+    m = int(min(n, max(cores, target_seconds * cores / per_cell)))
+    stride = max(1, n // m)
+    idx = np.arange(sample_offset % stride, n, stride)[:m]
+    r = refrun.integrate(case, wl.T[idx], wl.p[idx], wl.rho[idx], wl.dt, wl.dt, wl.Y[:, idx],
+                         procs=cores, workdir=work)
+    secs = r["seconds"]
+    return idx.size / secs, int(idx.size), secs
+
+
+# ----------------------------------------------------------------------------- GPU arm
+def run_ours(args, ws, rank, local):
+    import torch
+    import ctypes as C
+    from openhurricane_b200 import _capi, workloads
+    from openhurricane_b200.chemistry import ChemistrySource, Flow, Mechanism, integrate_host
+
+    if not torch.cuda.is_available():
+        raise RuntimeError("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=dev)
+
+    name = args.workload
+    ncells = args.cells or WORKLOAD_CELLS[name]
+    # the mechanism for the near-equilibrium relaxation of the batched pool
+    relax_mech = {}
+    if name == "batched":
+        _, _, t_small = workloads.mechanism_files("small")
+        relax_mech["mech"] = Mechanism(t_small)
+    wl = build_workload(name, ncells, seed_offset=rank, relax_mech=relax_mech)
+    mech = Mechanism(wl.tables)
+    if args.kernel is not None:
+        mech.set_tuning(args.kernel, args.block)
+    n, nsp = wl.n, wl.tables.nsp
+    d = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+    T0, p0, rho0, Y0 = d(wl.T), d(wl.p), d(wl.rho), d(wl.Y)
+    flow = Flow(T0.clone(), p0, rho0.clone(), Y0.clone())
+    cs = ChemistrySource(mech, flow, **workloads.SOLVER_OPTS)
+    dt = torch.full((n,), wl.dt, dtype=torch.float64, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def restore():
+        flow.T.copy_(T0)
+        flow.rho.copy_(rho0)
+        flow.Y.copy_(Y0)
+        cs.dtInit = None
+
+    # warm-up: the first call also fixes the stiffness order for later steps
+    counters = None
+    for w in range(args.warmup):
+        restore()
+        cs.solveUpdate(dt, 1.0, counters=(w == args.warmup - 1))
+    torch.cuda.synchronize()
+    counters = dict(cs.last_counters)
+
+    fm = workloads.flop_model(wl.tables)
+    flops_per_launch = workloads.work_flops(counters, fm)
+
+    clocks = ClockSampler(local)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for k in range(args.steps):
+        restore()
+        flush.fill_(float(k))
+        ev[k][0].record(stream)
+        cs.solveUpdate(dt, 1.0)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    ms_local = float(sum(step_ms))
+
+    # kernel-only timing of the integrator launch (the roofline's denominator)
+    lib = _capi.load()
+    kev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    restore()
+    flush.fill_(-1.0)
+    kev[0].record(stream)
+    rc = lib.hc_integrate_ordered(mech.handle, C.byref(cs.opts), n, C.c_void_p(flow.T.data_ptr()),
+                                  C.c_void_p(flow.p.data_ptr()), C.c_void_p(flow.rho.data_ptr()),
+                                  C.c_void_p(flow.Y.data_ptr()), C.c_void_p(dt.data_ptr()), 1.0,
+                                  C.c_void_p(cs._dt_init(dt, 1.0).data_ptr()), None,
+                                  C.c_void_p(cs.status.data_ptr()),
+                                  C.c_void_p(cs.order.data_ptr()) if cs.order is not None else None,
+                                  C.c_void_p(cs.cost.data_ptr()), None,
+                                  C.c_void_p(stream.cuda_stream))
+    kev[1].record(stream)
+    _capi.check(rc, "hc_integrate_ordered")
+    torch.cuda.synchronize()
+    kernel_ms = kev[0].elapsed_time(kev[1])
+    clk = clocks.stop()
+
+    # end to end: host (pinned) buffers through hc_integrate_host
+    pin = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64).pin_memory()
+    hT0, hrho0, hY0 = wl.T.copy(), wl.rho.copy(), np.ascontiguousarray(wl.Y)
+    hT, hp, hrho, hY = pin(wl.T), pin(wl.p), pin(wl.rho), pin(wl.Y)
+    hdt, hsub = pin(np.full(n, wl.dt)), pin(np.full(n, wl.dt))
+    hst = torch.zeros(n, dtype=torch.int32).pin_memory()
+    vp = lambda t: C.c_void_p(t.data_ptr())
+    e2e_steps = max(1, min(args.steps, 5))
+
+    def host_call():
+        o = cs.opts
+        r = lib.hc_integrate_host(mech.handle, C.byref(o), n, vp(hT), vp(hp), vp(hrho), vp(hY),
+                                  vp(hdt), 1.0, vp(hsub), None, vp(hst), None,
+                                  C.c_void_p(stream.cuda_stream))
+        _capi.check(r, "hc_integrate_host")
+
+    def host_restore():
+        hT.numpy()[:] = hT0
+        hrho.numpy()[:] = hrho0
+        hY.numpy()[:] = hY0
+        hsub.numpy()[:] = wl.dt
+
+    host_restore()
+    host_call()
+    torch.cuda.synchronize()
+    e2e_ms = 0.0
+    for k in range(e2e_steps):
+        host_restore()
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        host_call()
+        b.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms += a.elapsed_time(b)
+    e2e_ms /= e2e_steps
+    h2d = n * (5 + nsp) * 8
+    d2h = n * (3 + nsp) * 8 + n * 4
+
+    # FP64 peak on this GPU
+    peak = C.c_double(0.0)
+    _capi.check(lib.hc_probe_fp64_peak(1 << 16, C.byref(peak), C.c_void_p(stream.cuda_stream)),
+                "hc_probe_fp64_peak")
+
+    from openhurricane_b200 import replicas
+    ms_total, e2e_ms = replicas.max_over_ranks([ms_local, e2e_ms], device=dev)
+    cells_all = replicas.sum_over_ranks([n], device=dev)[0]
+    ms_step = ms_total / args.steps
+    value = replicas.whole_job_rate([cells_all], ms_step)
+
+    out = None
+    if rank == 0:
+        achieved = flops_per_launch / (kernel_ms * 1e-3) / 1e12
+        cores = _host_cores()
+        cpu = None
+        if not args.no_cpu_baseline:
+            cb = reference_cpu(wl, args.cpu_seconds, cores)
+            if cb is not None:
+                v, m, secs = cb
+                cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
+                       "sample": f"{m} of {n} cells (strided), reference ImplicitEuler, "
+                                 f"{cores} single-threaded processes, {secs:.1f} s"}
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded)", "impl": "ours",
+            "config": dict(workload_config(wl, name), parallelism=f"replicas x{ws}"),
+            "e2e": {"value": replicas.whole_job_rate([cells_all], e2e_ms), "unit": UNIT,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak.value,
+                         "unit": "TFLOP/s", "frac": achieved / peak.value,
+                         "traffic": None,
+                         "peak_source": "FP64 FMA probe measured in this run "
+                                        "(no FP64 figure in the measured peaks file)",
+                         "kernel_ms": kernel_ms, "flops_per_launch": flops_per_launch},
+            "counters": counters,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+def run_reference(args, ws, rank):
+    """Reference CPU integrator on the host cores; rank 0 only."""
+    if rank != 0:
+        return None
+    from oracle import refrun
+    from openhurricane_b200 import workloads
+    name = args.workload
+    ncells = args.cells or WORKLOAD_CELLS[name]
+    if not refrun.available():
+        return {"impl": "reference", "unavailable": "reference CPU binary oracle/_ref/hurchem_ref "
+                                                    "not built (make -f oracle/Makefile.ref)"}
+    cores = _host_cores()
+    if name == "batched":
+        # the near-equilibrium pool is relaxed by the reference integrator itself
+        def relax(T, p, rho, Y, t_relax):
+            case = os.path.join(work, "relax.cont")
+            refrun.write_case(case, *files, dict(workloads.SOLVER_OPTS))
+            r = refrun.integrate(case, T, p, rho, t_relax, t_relax, Y, procs=cores, workdir=work)
+            return r["T"], r["rho"], r["Y"]
+        work = tempfile.mkdtemp(prefix="hc_refrelax_")
+        _, files, _ = workloads.mechanism_files("small", os.path.join(work, "mech"))
+        wl = workloads.make_batched(ncells, seed=2002, relax=relax)
+    elif name == "small":
+        wl = workloads.make_small(ncells)
+    else:
+        wl = workloads.make_large(ncells)
+    budget = max(2.0, min(20.0, 150.0 / max(1, args.steps + args.warmup)))
+    for w in range(args.warmup):
+        reference_cpu(wl, min(budget, 2.0), cores, sample_offset=w)
+    vals, cells, secs = [], 0, 0.0
+    for k in range(args.steps):
+        v, m, s = reference_cpu(wl, budget, cores, sample_offset=args.warmup + k)
+        vals.append(v)
+        cells += m
+        secs += s
+    value = cells / secs
+    return {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)", "impl": "reference",
+        "config": dict(workload_config(wl, name), parallelism="host cores"),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"each step a strided sample of ~{cells // args.steps} of "
+                                   f"{wl.n} cells, {cores} single-threaded processes"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "gpu_launches": 0,
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOAD_CELLS), default="batched")
+    ap.add_argument("--cells", type=int, default=0)
+    ap.add_argument("--kernel", type=int, default=None, help="0 auto, 1 thread/cell, 2 group")
+    ap.add_argument("--block", type=int, default=64)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 1:
+        raise SystemExit("--warmup must be >= 1")
+    ws, rank, local = _dist()
+    if args.impl == "reference":
+        out = run_reference(args, ws, rank)
+    else:
+        out = run_ours(args, ws, rank, local)
+    if out is not None and rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -216,6 +216,20 @@ int hc_properties(hc_mech_t mech, int64_t n, const double *T, const double *p, c
                   double *ha, double *cp, double *mu, double *kappa, double *D, void *stream);
 
 /*
+ * Host-buffer forms of hc_source_terms and hc_properties: copy in, compute,
+ * copy out, synchronise the stream. They serve the reference's host-side
+ * callers, which pass host arrays: chemistrySource::calculateSourceTerms
+ * (chemistrySource.cpp:1370-1406), CUDAThermo::calchaicp
+ * (thermo/include/thermoListCUDA.hpp:40-58) and
+ * CUDATransport::calcTransportProperties (transport/src/transportListCUDA.cu:236).
+ */
+int hc_source_terms_host(hc_mech_t mech, int64_t n, const double *T, const double *p,
+                         const double *rho, const double *Y, double *Ri, void *stream);
+int hc_properties_host(hc_mech_t mech, int64_t n, const double *T, const double *p,
+                       const double *Y, double *ha, double *cp, double *mu, double *kappa,
+                       double *D, void *stream);
+
+/*
  * Measurement utility, no reference counterpart: runs an FP64 FMA-throughput
  * probe on the current device (independent FMA chains on every SM) and
  * returns the achieved TFLOP/s, the denominator of the integrator's roofline.

@@ -388,6 +388,19 @@ static int integrate_impl(hc_mech_t m, const hc_opts *opts, int64_t ncells, doub
     HC_DISPATCH(m, integrate, m->dm, m->num_sms, P, io, st, g_err);
 }
 
+// grow the host-entry-point workspace (callers hold m->mu); growing
+// synchronises the stream first
+static int ensure_ws(hc_mech_t m, size_t bytes, cudaStream_t st) {
+    if (m->ws_bytes >= bytes) return HC_OK;
+    HC_CUDA(cudaStreamSynchronize(st));
+    if (m->ws) cudaFree(m->ws);
+    m->ws = nullptr;
+    m->ws_bytes = 0;
+    HC_CUDA(cudaMalloc(&m->ws, bytes));
+    m->ws_bytes = bytes;
+    return HC_OK;
+}
+
 static int read_counters(hc_mech_t m, hc_counters *c, cudaStream_t st) {
     if (!c) return HC_OK;
     unsigned long long h[7];
@@ -446,14 +459,8 @@ int hc_integrate_host(hc_mech_t m, const hc_opts *opts, int64_t ncells, double *
     const int nsp = m->dm.nsp;
     const size_t n = (size_t)ncells;
     const size_t bytes = sizeof(double) * (n * (5 + 2 * (size_t)nsp)) + sizeof(int32_t) * n + 256;
-    if (m->ws_bytes < bytes) {
-        HC_CUDA(cudaStreamSynchronize(st));
-        if (m->ws) cudaFree(m->ws);
-        m->ws = nullptr;
-        m->ws_bytes = 0;
-        HC_CUDA(cudaMalloc(&m->ws, bytes));
-        m->ws_bytes = bytes;
-    }
+    int wrc = ensure_ws(m, bytes, st);
+    if (wrc != HC_OK) return wrc;
     double *dT = static_cast<double *>(m->ws);
     double *dp = dT + n, *drho = dp + n, *ddt = drho + n, *dsub = ddt + n;
     double *dY = dsub + n, *dRi = dY + n * nsp;
@@ -512,6 +519,58 @@ int hc_properties(hc_mech_t m, int64_t n, const double *T, const double *p, cons
         return fail(HC_E_INVALID, "mechanism has no transport data");
     return launch_properties(m->dm, n, T, p, Y, ha, cp, mu, kappa, D,
                              static_cast<cudaStream_t>(stream), g_err);
+}
+
+int hc_source_terms_host(hc_mech_t m, int64_t n, const double *T, const double *p,
+                         const double *rho, const double *Y, double *Ri, void *stream) {
+    if (!m) return fail(HC_E_INVALID, "null mechanism");
+    if (n <= 0) return HC_OK;
+    if (!T || !p || !rho || !Y || !Ri) return fail(HC_E_INVALID, "null field");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    std::lock_guard<std::mutex> lk(m->mu);
+    const size_t nn = (size_t)n, nsp = (size_t)m->dm.nsp;
+    int rc = ensure_ws(m, sizeof(double) * nn * (3 + 2 * nsp), st);
+    if (rc != HC_OK) return rc;
+    double *dT = static_cast<double *>(m->ws), *dp = dT + nn, *dr = dp + nn, *dY = dr + nn;
+    double *dR = dY + nn * nsp;
+    HC_CUDA(cudaMemcpyAsync(dT, T, sizeof(double) * nn, cudaMemcpyHostToDevice, st));
+    HC_CUDA(cudaMemcpyAsync(dp, p, sizeof(double) * nn, cudaMemcpyHostToDevice, st));
+    HC_CUDA(cudaMemcpyAsync(dr, rho, sizeof(double) * nn, cudaMemcpyHostToDevice, st));
+    HC_CUDA(cudaMemcpyAsync(dY, Y, sizeof(double) * nn * nsp, cudaMemcpyHostToDevice, st));
+    rc = hc_source_terms(m, n, dT, dp, dr, dY, dR, stream);
+    if (rc != HC_OK) return rc;
+    HC_CUDA(cudaMemcpyAsync(Ri, dR, sizeof(double) * nn * nsp, cudaMemcpyDeviceToHost, st));
+    HC_CUDA(cudaStreamSynchronize(st));
+    return HC_OK;
+}
+
+int hc_properties_host(hc_mech_t m, int64_t n, const double *T, const double *p, const double *Y,
+                       double *ha, double *cp, double *mu, double *kappa, double *D,
+                       void *stream) {
+    if (!m) return fail(HC_E_INVALID, "null mechanism");
+    if (n <= 0) return HC_OK;
+    if (!T || !p || !Y) return fail(HC_E_INVALID, "null field");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    std::lock_guard<std::mutex> lk(m->mu);
+    const size_t nn = (size_t)n, nsp = (size_t)m->dm.nsp;
+    int rc = ensure_ws(m, sizeof(double) * nn * (5 + 3 * nsp), st);
+    if (rc != HC_OK) return rc;
+    double *dT = static_cast<double *>(m->ws), *dp = dT + nn, *dY = dp + nn;
+    double *dha = dY + nn * nsp, *dD = dha + nn * nsp, *dcp = dD + nn * nsp, *dmu = dcp + nn;
+    double *dk = dmu + nn;
+    HC_CUDA(cudaMemcpyAsync(dT, T, sizeof(double) * nn, cudaMemcpyHostToDevice, st));
+    HC_CUDA(cudaMemcpyAsync(dp, p, sizeof(double) * nn, cudaMemcpyHostToDevice, st));
+    HC_CUDA(cudaMemcpyAsync(dY, Y, sizeof(double) * nn * nsp, cudaMemcpyHostToDevice, st));
+    rc = hc_properties(m, n, dT, dp, dY, ha ? dha : nullptr, cp ? dcp : nullptr,
+                       mu ? dmu : nullptr, kappa ? dk : nullptr, D ? dD : nullptr, stream);
+    if (rc != HC_OK) return rc;
+    if (ha) HC_CUDA(cudaMemcpyAsync(ha, dha, sizeof(double) * nn * nsp, cudaMemcpyDeviceToHost, st));
+    if (D) HC_CUDA(cudaMemcpyAsync(D, dD, sizeof(double) * nn * nsp, cudaMemcpyDeviceToHost, st));
+    if (cp) HC_CUDA(cudaMemcpyAsync(cp, dcp, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
+    if (mu) HC_CUDA(cudaMemcpyAsync(mu, dmu, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
+    if (kappa) HC_CUDA(cudaMemcpyAsync(kappa, dk, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
+    HC_CUDA(cudaStreamSynchronize(st));
+    return HC_OK;
 }
 
 }  // extern "C"

@@ -106,8 +106,18 @@ def _p(a):
     return a.ctypes.data
 
 
+def _threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
 def integrate(md: MechDesc, T, p, rho, Y, dt, subdt=None, dt_factor=1.0,
-              opts: Optional[HcOpts] = None) -> Dict[str, np.ndarray]:
+              opts: Optional[HcOpts] = None, threads: Optional[int] = None) -> Dict[str, np.ndarray]:
+    """Integrate every cell (the C restatement is re-entrant; cells are split
+    into contiguous slices over `threads` host threads, ctypes releasing the
+    GIL during each call)."""
     n = int(np.asarray(T).shape[0])
     T = np.array(T, dtype=np.float64, copy=True)
     p = np.ascontiguousarray(np.broadcast_to(np.asarray(p, np.float64), (n,)))
@@ -118,12 +128,35 @@ def integrate(md: MechDesc, T, p, rho, Y, dt, subdt=None, dt_factor=1.0,
                    dtype=np.float64, copy=True)
     c = np.zeros_like(Y)
     st = np.zeros(n, np.int32)
-    cnt = HcCounters()
     o = opts or default_opts()
-    rc = lib().oracle_integrate(C.byref(md.desc), C.byref(o), n, _p(T), _p(p), _p(rho), _p(Y),
-                                _p(dt), dt_factor, _p(sub), _p(c), _p(st), C.addressof(cnt))
+    nth = max(1, min(threads or _threads(), n))
+    bounds = np.linspace(0, n, nth + 1).astype(np.int64)
+    L = lib()
+
+    def one(k):
+        a, b = int(bounds[k]), int(bounds[k + 1])
+        if b <= a:
+            return 0, HcCounters()
+        Ts, ps, rs = T[a:b].copy(), p[a:b].copy(), rho[a:b].copy()
+        Ys, ds, ss = np.ascontiguousarray(Y[:, a:b]), dt[a:b].copy(), sub[a:b].copy()
+        cs, sts = np.zeros_like(Ys), np.zeros(b - a, np.int32)
+        cnt = HcCounters()
+        rc = L.oracle_integrate(C.byref(md.desc), C.byref(o), b - a, _p(Ts), _p(ps), _p(rs),
+                                _p(Ys), _p(ds), dt_factor, _p(ss), _p(cs), _p(sts),
+                                C.addressof(cnt))
+        T[a:b], rho[a:b], Y[:, a:b], sub[a:b], c[:, a:b], st[a:b] = Ts, rs, Ys, ss, cs, sts
+        return rc, cnt
+
+    if nth == 1:
+        parts = [one(0)]
+    else:
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(max_workers=nth) as ex:
+            parts = list(ex.map(one, range(nth)))
+    rc = sum(r for r, _ in parts)
+    counters = {k: int(sum(getattr(cn, k) for _, cn in parts)) for k, _ in HcCounters._fields_}
     return {"T": T, "rho": rho, "Y": Y, "c": c, "subdt": sub, "status": st, "rc": rc,
-            "counters": {k: getattr(cnt, k) for k, _ in HcCounters._fields_}}
+            "counters": counters}
 
 
 def rhs_jac(md: MechDesc, c, T):
