@@ -185,6 +185,17 @@ int hc_integrate_ordered(hc_mech_t mech, const hc_opts *opts, int64_t ncells, do
                          const int32_t *order, int64_t *cost, hc_counters *counters,
                          void *stream);
 
+/*
+ * Integrate only the cells sel[0..nsel) of fields of length ncells (device
+ * pointers; species fields keep the stride ncells); other cells are not
+ * touched. Used for the surrogate's rejected cells. No reference
+ * counterpart.
+ */
+int hc_integrate_subset(hc_mech_t mech, const hc_opts *opts, int64_t ncells, int64_t nsel,
+                        const int32_t *sel, double *T, const double *p, double *rho, double *Y,
+                        const double *dt, double dt_factor, double *subdt, double *Ri,
+                        int32_t *status, int64_t *cost, hc_counters *counters, void *stream);
+
 /* Same as hc_integrate with host buffers: H2D, integrate, D2H, synchronise. */
 int hc_integrate_host(hc_mech_t mech, const hc_opts *opts, int64_t ncells, double *T,
                       const double *p, double *rho, double *Y, const double *dt, double dt_factor,
@@ -235,6 +246,71 @@ int hc_properties_host(hc_mech_t mech, int64_t n, const double *T, const double 
  * returns the achieved TFLOP/s, the denominator of the integrator's roofline.
  */
 int hc_probe_fp64_peak(int iters, double *tflops, void *stream);
+
+/* ------------------------------------------------------------------------
+ * Surrogate network (no reference counterpart): a multilayer perceptron
+ * n_in -> n_hidden x width (GELU) -> n_out with BF16 tensor-core (tcgen05)
+ * forward and backward kernels accumulating in FP32, FP32 master parameters
+ * and Adam. Inputs and targets are device fp32 row-major [B][n_in] /
+ * [B][n_out], already normalised by the caller. Errors are reported through
+ * hc_last_error().
+ */
+typedef struct hc_mlp_s *hc_mlp_t;
+
+int hc_mlp_create(int n_in, int n_out, int n_hidden, int width, int max_batch, uint64_t seed,
+                  hc_mlp_t *out);
+int hc_mlp_destroy(hc_mlp_t mlp);
+int64_t hc_mlp_num_params(hc_mlp_t mlp);
+/* host parameter layout, layer by layer: W [out][in] row-major, then b [out] */
+int hc_mlp_get_params(hc_mlp_t mlp, float *host);
+int hc_mlp_set_params(hc_mlp_t mlp, const float *host);
+/* gradients of the mean-squared error (parameter layout), no update; synchronises */
+int hc_mlp_grad(hc_mlp_t mlp, const float *X, const float *Y, int B, float *grad_host,
+                float *loss_host, void *stream);
+/* one Adam step; loss_host != NULL or check != 0 make the call synchronous */
+int hc_mlp_train_step(hc_mlp_t mlp, const float *X, const float *Y, int B, float lr,
+                      float *loss_host, int check, void *stream);
+/* Y = net(X) for any B (processed in chunks of max_batch rows) */
+int hc_mlp_forward(hc_mlp_t mlp, const float *X, int64_t B, float *Y, void *stream);
+/* reads and clears the tensor-core pipelines' timeout flag; synchronises */
+int hc_mlp_check(hc_mlp_t mlp, void *stream);
+/* test entry: C[M][N] = act(A[M][K] B[N][K]^T + bias), bf16 in, fp32 out,
+ * M % 128 == 0, N % 32 == 0, K % 64 == 0; act 0 identity, 1 GELU */
+int hc_gemm_bf16_tn(const void *A, const void *B, int M, int N, int K, const float *bias,
+                    int act, float *C, void *stream);
+
+/*
+ * Surrogate path around the network (no reference counterpart).
+ *
+ * hc_surrogate_features: X[n][nsp+3] (float) = normalised (T, ln p, Y_1..Y_nsp,
+ * ln(dt*dt_factor)): (value - mean[j]) * inv_std[j].
+ *
+ * hc_surrogate_gate: pred[n][nsp+1] is the network's normalised increment
+ * (dT, dY_1..dY_nsp) over the flow step (de-normalised with out_mean /
+ * out_std). Per cell, in FP64: dY is projected onto the element-conserving
+ * subspace with proj[nsp][nsp]; Y' = Y + dY (components below -y_neg reject,
+ * those in [-y_neg, 0) become 0); T' solves sum Y'_i h_i(T') = sum Y_i h_i(T)
+ * (constant-pressure enthalpy); the cell is accepted when |T' - (T + dT)| <=
+ * tol_T, the projection moved dY by at most tol_proj * max(|dY|_inf, 1e-6),
+ * every |X| <= x_max and T_min < T' < T_max. Accepted cells get T', Y' and
+ * rho = p/(R_m T'); rejected cells are untouched, listed in rejected[0..
+ * *n_rejected) (any order) for hc_integrate_subset. Synchronises the stream.
+ */
+typedef struct hc_gate_opts {
+    double tol_T;     /* K */
+    double tol_proj;  /* relative */
+    double y_neg;     /* largest negative mass fraction clipped to zero */
+    double x_max;     /* input features' range, in training standard deviations */
+    double T_min, T_max;
+} hc_gate_opts;
+
+int hc_surrogate_features(hc_mech_t mech, int64_t n, const double *T, const double *p,
+                          const double *Y, const double *dt, double dt_factor, const double *mean,
+                          const double *inv_std, float *X, void *stream);
+int hc_surrogate_gate(hc_mech_t mech, int64_t n, double *T, const double *p, double *rho,
+                      double *Y, const float *pred, const float *X, const double *out_mean,
+                      const double *out_std, const double *proj, const hc_gate_opts *gate,
+                      int32_t *accept, int32_t *rejected, int64_t *n_rejected, void *stream);
 
 #ifdef __cplusplus
 }

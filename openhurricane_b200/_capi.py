@@ -47,6 +47,11 @@ class HcOpts(C.Structure):
     ]
 
 
+class HcGateOpts(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("tol_T", "tol_proj", "y_neg", "x_max", "T_min",
+                                          "T_max")]
+
+
 class HcCounters(C.Structure):
     _fields_ = [(k, C.c_int64) for k in ("n_jac", "n_rhs", "n_lu", "n_newton", "n_steps",
                                          "n_attempts")]
@@ -70,6 +75,8 @@ SIGNATURES = {
                      [_VP] * 4 + [_VP]),
     "hc_integrate_ordered": (C.c_int, [_VP, C.POINTER(HcOpts), C.c_int64] + [_VP] * 5 +
                              [C.c_double] + [_VP] * 6 + [_VP]),
+    "hc_integrate_subset": (C.c_int, [_VP, C.POINTER(HcOpts), C.c_int64, C.c_int64, _VP] +
+                            [_VP] * 5 + [C.c_double] + [_VP] * 5 + [_VP]),
     "hc_integrate_host": (C.c_int, [_VP, C.POINTER(HcOpts), C.c_int64] + [_VP] * 5 +
                           [C.c_double] + [_VP] * 4 + [_VP]),
     "hc_rhs_jacobian": (C.c_int, [_VP, C.c_int64] + [_VP] * 5 + [_VP]),
@@ -78,6 +85,18 @@ SIGNATURES = {
     "hc_source_terms_host": (C.c_int, [_VP, C.c_int64] + [_VP] * 5 + [_VP]),
     "hc_properties_host": (C.c_int, [_VP, C.c_int64] + [_VP] * 8 + [_VP]),
     "hc_probe_fp64_peak": (C.c_int, [C.c_int, _VP, _VP]),
+    "hc_mlp_create": (C.c_int, [C.c_int] * 5 + [C.c_uint64, C.POINTER(_VP)]),
+    "hc_mlp_destroy": (C.c_int, [_VP]),
+    "hc_mlp_num_params": (C.c_int64, [_VP]),
+    "hc_mlp_get_params": (C.c_int, [_VP, _VP]),
+    "hc_mlp_set_params": (C.c_int, [_VP, _VP]),
+    "hc_mlp_grad": (C.c_int, [_VP, _VP, _VP, C.c_int, _VP, _VP, _VP]),
+    "hc_mlp_train_step": (C.c_int, [_VP, _VP, _VP, C.c_int, C.c_float, _VP, C.c_int, _VP]),
+    "hc_mlp_forward": (C.c_int, [_VP, _VP, C.c_int64, _VP, _VP]),
+    "hc_mlp_check": (C.c_int, [_VP, _VP]),
+    "hc_surrogate_features": (C.c_int, [_VP, C.c_int64] + [_VP] * 4 + [C.c_double] + [_VP] * 4),
+    "hc_surrogate_gate": (C.c_int, [_VP, C.c_int64] + [_VP] * 14),
+    "hc_gemm_bf16_tn": (C.c_int, [_VP, _VP, C.c_int, C.c_int, C.c_int, _VP, C.c_int, _VP, _VP]),
 }
 
 _lib: Optional[C.CDLL] = None

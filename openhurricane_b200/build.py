@@ -21,7 +21,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC"]
 # translation units: the C ABI plus one file per kernel variant
 UNITS = ["capi.cu", "variant_10.cu", "variant_16.cu", "variant_32.cu", "variant_54.cu",
-         "variant_64.cu", "variant_t1.cu", "props.cu", "probe.cu"]
+         "variant_64.cu", "variant_t1.cu", "props.cu", "probe.cu", "mlp.cu", "surrogate.cu"]
 
 
 def nvcc() -> str:

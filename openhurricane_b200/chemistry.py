@@ -161,8 +161,13 @@ class ChemistrySource:
         if cnt is not None:
             self.last_counters = cnt.as_dict()
         if self.rebin:
-            # stiffest cells first on the next flow step
-            self.order = torch.argsort(self.cost, descending=True).to(torch.int32)
+            # stiffest cells first on the next flow step; updated in place so
+            # that a captured graph's launch reads the new order on replay
+            new_order = torch.argsort(self.cost, descending=True).to(torch.int32)
+            if self.order is None:
+                self.order = new_order
+            else:
+                self.order.copy_(new_order)
 
     def solve(self, dt: torch.Tensor, dt_factor: float = 1.0, counters: bool = False) -> float:
         """Integrate every cell over dt*dtFactor and fill Ri; the flow fields
@@ -179,6 +184,26 @@ class ChemistrySource:
         """Integrate every cell and write Y, T back (chemistrySource::solveUpdate)."""
         f = self.flow
         self._integrate(dt, dt_factor, f.T, f.rho, f.Y, None, counters)
+
+    def capture_update(self, dt: torch.Tensor, dt_factor: float = 1.0) -> "torch.cuda.CUDAGraph":
+        """Capture one solveUpdate flow step (queue reset, integrator launch
+        and the stiffness re-ordering) in a CUDA graph; replaying it advances
+        the flow fields in place. dt, the fields, dtInit and the order buffer
+        must stay allocated while the graph is used. A solveUpdate (or solve)
+        on these fields must have run first: it sizes the library's per-cell
+        buffers (growing them synchronises the stream, which capture forbids)
+        and creates the order buffer."""
+        if self.dtInit is None or (self.rebin and self.order is None):
+            raise RuntimeError("run solveUpdate once before capturing")
+        f = self.flow
+        g = torch.cuda.CUDAGraph()
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            with torch.cuda.graph(g, stream=side):
+                self._integrate(dt, dt_factor, f.T, f.rho, f.Y, None, False)
+        torch.cuda.current_stream().wait_stream(side)
+        return g
 
     def calculateSourceTerms(self, withoutLastSpec: bool = False):
         """Ri = omega_i W_i at the current state (chemistrySource::calculateSourceTerms)."""

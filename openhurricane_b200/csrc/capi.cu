@@ -17,13 +17,24 @@
 #include <vector>
 
 #include "../../include/hurchem_b200.h"
+#include "surrogate.cuh"
 #include "variants.h"
 
 using namespace hc;
 
+
 namespace {
 
 thread_local std::string g_err;
+
+}  // namespace
+
+namespace hc {
+// the message hc_last_error() returns, shared by every translation unit
+void set_last_error(const std::string &msg) { g_err = msg; }
+}  // namespace hc
+
+namespace {
 
 int fail(int code, const std::string &msg) {
     g_err = msg;
@@ -341,7 +352,8 @@ int hc_mech_nrc(hc_mech_t m) { return m ? m->dm.nrc : -1; }
 static int integrate_impl(hc_mech_t m, const hc_opts *opts, int64_t ncells, double *T,
                           const double *p, double *rho, double *Y, const double *dt,
                           double dt_factor, double *subdt, double *Ri, int32_t *status,
-                          const int32_t *order, int64_t *cost, cudaStream_t st) {
+                          const int32_t *order, int64_t *cost, cudaStream_t st,
+                          int64_t nqueue = -1) {
     if (!m) return fail(HC_E_INVALID, "null mechanism");
     int rc = check_opts(opts);
     if (rc != HC_OK) return rc;
@@ -353,6 +365,10 @@ static int integrate_impl(hc_mech_t m, const hc_opts *opts, int64_t ncells, doub
     const IntegratorParams P = make_params(opts);
     CellIO io;
     io.ncells = ncells;
+    io.nqueue = (nqueue < 0) ? ncells : nqueue;
+    if (io.nqueue > ncells || (nqueue >= 0 && !order))
+        return fail(HC_E_INVALID, "subset needs a cell list no longer than the fields");
+    if (io.nqueue == 0) return HC_OK;
     io.T = T;
     io.p = p;
     io.rho = rho;
@@ -442,6 +458,19 @@ int hc_integrate_ordered(hc_mech_t m, const hc_opts *opts, int64_t ncells, doubl
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     int rc = integrate_impl(m, opts, ncells, T, p, rho, Y, dt, dt_factor, subdt, Ri, status,
                             order, cost, st);
+    if (rc != HC_OK) return rc;
+    return read_counters(m, counters, st);
+}
+
+int hc_integrate_subset(hc_mech_t m, const hc_opts *opts, int64_t ncells, int64_t nsel,
+                        const int32_t *sel, double *T, const double *p, double *rho, double *Y,
+                        const double *dt, double dt_factor, double *subdt, double *Ri,
+                        int32_t *status, int64_t *cost, hc_counters *counters, void *stream) {
+    if (nsel < 0) return fail(HC_E_INVALID, "negative subset size");
+    if (nsel > 0 && !sel) return fail(HC_E_INVALID, "null cell list");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int rc = integrate_impl(m, opts, ncells, T, p, rho, Y, dt, dt_factor, subdt, Ri, status, sel,
+                            cost, st, nsel);
     if (rc != HC_OK) return rc;
     return read_counters(m, counters, st);
 }
@@ -570,6 +599,59 @@ int hc_properties_host(hc_mech_t m, int64_t n, const double *T, const double *p,
     if (mu) HC_CUDA(cudaMemcpyAsync(mu, dmu, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
     if (kappa) HC_CUDA(cudaMemcpyAsync(kappa, dk, sizeof(double) * nn, cudaMemcpyDeviceToHost, st));
     HC_CUDA(cudaStreamSynchronize(st));
+    return HC_OK;
+}
+
+int hc_surrogate_features(hc_mech_t m, int64_t n, const double *T, const double *p,
+                          const double *Y, const double *dt, double dt_factor, const double *mean,
+                          const double *inv_std, float *X, void *stream) {
+    if (!m) return fail(HC_E_INVALID, "null mechanism");
+    if (n <= 0) return HC_OK;
+    if (!T || !p || !Y || !dt || !mean || !inv_std || !X) return fail(HC_E_INVALID, "null field");
+    return launch_features(m->dm, n, T, p, Y, dt, dt_factor, mean, inv_std, X,
+                           static_cast<cudaStream_t>(stream));
+}
+
+int hc_surrogate_gate(hc_mech_t m, int64_t n, double *T, const double *p, double *rho, double *Y,
+                      const float *pred, const float *X, const double *out_mean,
+                      const double *out_std, const double *proj, const hc_gate_opts *g,
+                      int32_t *accept, int32_t *rejected, int64_t *n_rejected, void *stream) {
+    if (!m) return fail(HC_E_INVALID, "null mechanism");
+    if (!g || !n_rejected) return fail(HC_E_INVALID, "null argument");
+    *n_rejected = 0;
+    if (n <= 0) return HC_OK;
+    if (!T || !p || !rho || !Y || !pred || !X || !out_mean || !out_std || !proj || !accept ||
+        !rejected)
+        return fail(HC_E_INVALID, "null field");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    unsigned long long *cnt = m->queue + 7;
+    HC_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), st));
+    GateArgs a;
+    a.n = n;
+    a.T = T;
+    a.p = p;
+    a.rho = rho;
+    a.Y = Y;
+    a.pred = pred;
+    a.X = X;
+    a.out_mean = out_mean;
+    a.out_std = out_std;
+    a.proj = proj;
+    a.tol_T = g->tol_T;
+    a.tol_proj = g->tol_proj;
+    a.y_neg = g->y_neg;
+    a.x_max = g->x_max;
+    a.T_min = g->T_min;
+    a.T_max = g->T_max;
+    a.accept = accept;
+    a.rejected = rejected;
+    a.n_rejected = cnt;
+    int rc = launch_gate(m->dm, a, st);
+    if (rc != HC_OK) return rc;
+    unsigned long long h = 0;
+    HC_CUDA(cudaMemcpyAsync(&h, cnt, sizeof(h), cudaMemcpyDeviceToHost, st));
+    HC_CUDA(cudaStreamSynchronize(st));
+    *n_rejected = (int64_t)h;
     return HC_OK;
 }
 

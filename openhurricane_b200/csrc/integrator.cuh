@@ -51,7 +51,8 @@ struct IntegratorParams {
 };
 
 struct CellIO {
-    int64_t ncells;
+    int64_t ncells;         // field length (stride of species fields)
+    int64_t nqueue;         // cells to integrate: queue entries 0..nqueue-1
     double *T;
     const double *p;
     double *rho;
@@ -701,7 +702,7 @@ integrate_kernel(const __grid_constant__ DevMech m, const __grid_constant__ Inte
         g.sync();
         const long long k = *slot;
         g.sync();
-        if (k >= io.ncells) break;
+        if (k >= io.nqueue) break;
         const int64_t cell = io.order ? (int64_t)io.order[k] : (int64_t)k;
         CellIntegrator<N, G> ci(m, P, g, s);
         const double Ti = io.T[cell];

@@ -476,7 +476,7 @@ integrate_t1_kernel(const __grid_constant__ DevMech m, const __grid_constant__ I
                     cellid = -1;
                 }
                 const unsigned long long k = atomicAdd(io.queue_head, 1ULL);
-                if ((long long)k >= io.ncells) {
+                if ((long long)k >= io.nqueue) {
                     state = kT1Done;
                     break;
                 }

@@ -101,7 +101,7 @@ def _cells(tables, n, seed, **kw):
     return c.T, c.p, synth.mixture_density(tables.W, c), c.Y
 
 
-@pytest.mark.parametrize("kernel,block", [(0, 64), (1, 32), (1, 128), (2, 32), (2, 64)])
+@pytest.mark.parametrize("kernel,block", [(0, 64), (1, 32), (1, 128), (2, 64)])
 def test_small_mechanism_parity_vs_oracle(small, kernel, block):
     t = small["tables"]
     T, p, rho, Y = _cells(t, 384, seed=11)
@@ -118,7 +118,7 @@ def test_small_mechanism_parity_vs_oracle(small, kernel, block):
     assert (np.abs(g["Ri"] - Ri_o) / scale).max() < 1e-5
 
 
-@pytest.mark.parametrize("kernel,block", [(0, 64), (2, 32)])
+@pytest.mark.parametrize("kernel,block", [(0, 64)])
 def test_large_mechanism_parity_vs_oracle(large, kernel, block):
     from openhurricane_b200 import workloads
     t = large["tables"]
@@ -270,3 +270,30 @@ def test_edge_cases(small):
     assert g0["T"].shape == (0,)
     # mass fractions stay normalised
     assert np.abs(g["Y"].sum(axis=0) - 1.0).max() < 1e-13
+
+
+@pytest.mark.parametrize("which", ["small", "large"])
+def test_graph_captured_step_matches_eager(which, small, large):
+    """A CUDA-graph replay of solveUpdate (queue reset, integrator launch,
+    stiffness re-ordering) gives the eager second flow step bit for bit."""
+    from openhurricane_b200.chemistry import ChemistrySource, Flow
+    dev = _cuda()
+    t = (small if which == "small" else large)["tables"]
+    n = 256 if which == "small" else 64
+    T, p, rho, Y = _cells(t, n, seed=123)
+    d = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+    m = _mech(t)
+    dt = torch.full((n,), 1e-6, dtype=torch.float64, device=dev)
+    fa = Flow(d(T), d(p), d(rho), d(Y))
+    a = ChemistrySource(m, fa)
+    a.solveUpdate(dt)
+    a.solveUpdate(dt)
+    fb = Flow(d(T), d(p), d(rho), d(Y))
+    b = ChemistrySource(m, fb)
+    b.solveUpdate(dt)
+    g = b.capture_update(dt)
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(fa.T, fb.T) and torch.equal(fa.Y, fb.Y) and torch.equal(fa.rho, fb.rho)
+    assert torch.equal(a.dtInit, b.dtInit)
+    del g
