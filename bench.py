@@ -271,6 +271,8 @@ def run_ours(args, ws, rank, local):
     torch.cuda.synchronize()
     kernel_ms = kev[0].elapsed_time(kev[1])
     clk = clocks.stop()
+    # the FP64 result of this step: the reference the surrogate is judged against
+    fp64_ref = (flow.T.clone(), flow.Y.clone())
 
     # end to end: host (pinned) buffers through hc_integrate_host
     pin = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64).pin_memory()
@@ -311,6 +313,11 @@ def run_ours(args, ws, rank, local):
     e2e_ms /= e2e_steps
     h2d = n * (5 + nsp) * 8
     d2h = n * (3 + nsp) * 8 + n * 4
+
+    sur = None
+    if args.surrogate and name == "batched":
+        sur = surrogate_leg(args, wl, mech, relax_mech["mech"], (T0, p0, rho0, Y0), dt, fp64_ref,
+                            ms_local / args.steps, flush, rank)
 
     # FP64 peak on this GPU
     peak = C.c_double(0.0)
@@ -353,11 +360,92 @@ def run_ours(args, ws, rank, local):
             "counters": counters,
             "clocks": clk,
             "cpu_baseline": cpu,
+            "surrogate": sur,
         }
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return out
+
+
+def surrogate_leg(args, wl, mech, relax_mech, fields0, dt, fp64_ref, plain_ms, flush, rank):
+    """Train the gated surrogate on samples of the FP64 GPU integrator (states
+    of the same distribution, another seed), then time its flow step on the
+    workload's cells and judge it against the FP64 step."""
+    import torch
+    from openhurricane_b200 import _capi, workloads
+    from openhurricane_b200.chemistry import Flow
+    from openhurricane_b200.surrogate import Surrogate, generate_samples, integrate_device
+    dev = fields0[0].device
+    opts = _capi.default_opts(**workloads.SOLVER_OPTS)
+    t0 = time.perf_counter()
+
+    def relax(T, p, rho, Y, tr):
+        d = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+        Td, pd, rd, Yd = d(T), d(p), d(rho), d(Y)
+        integrate_device(relax_mech, Td, pd, rd, Yd, torch.full_like(Td, tr), opts)
+        return Td.cpu().numpy(), rd.cpu().numpy(), Yd.cpu().numpy()
+
+    base = workloads.make_batched(65536, seed=5005 + rank, relax=relax)
+    d = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+    smp = generate_samples(mech, d(base.T), d(base.p), d(base.rho), d(base.Y), wl.dt,
+                           args.sur_samples, seed=11 + rank, opts=opts)
+    torch.cuda.synchronize()
+    t_gen = time.perf_counter() - t0
+    sur = Surrogate(mech, n_hidden=3, width=256, max_batch=65536, seed=3 + rank)
+    sur.fit_normalisation(smp["T"], smp["p"], smp["Y"], smp["dt"], smp["dT"], smp["dY"])
+    X = sur.features(smp["T"], smp["p"], smp["Y"], smp["dt"])
+    D = sur.targets(smp["dT"], smp["dY"])
+    n_train = int(X.shape[0])
+    del smp
+    t1 = time.perf_counter()
+    losses = sur.train(X, D, epochs=args.sur_epochs, batch=8192, lr=2e-3)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t1
+    del X, D
+    T0, p0, rho0, Y0 = fields0
+    n = int(T0.shape[0])
+    flow = Flow(T0.clone(), p0, rho0.clone(), Y0.clone())
+    stream = torch.cuda.current_stream()
+
+    def restore():
+        flow.T.copy_(T0)
+        flow.rho.copy_(rho0)
+        flow.Y.copy_(Y0)
+
+    restore()
+    sur.step(flow, dt, opts=opts)     # warm-up
+    ms, rej = [], []
+    for k in range(args.steps):
+        restore()
+        flush.fill_(float(k))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        nr, accept = sur.step(flow, dt, opts=opts)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+        rej.append(nr)
+    Tref, Yref = fp64_ref
+    acc = accept.bool()
+    dT = (flow.T - Tref).abs()
+    dY = (flow.Y - Yref).abs()
+    A = torch.tensor(wl.tables.elem_matrix / wl.tables.W[None, :], dtype=torch.float64, device=dev)
+    e0, e1 = A @ Y0, A @ flow.Y
+    rel = ((e1 - e0).abs() / e0.abs().max(dim=0, keepdim=True).values)
+    sur_ms = float(np.mean(ms))
+    return {"cells_per_s": n / (sur_ms * 1e-3), "ms_per_step": sur_ms,
+            "speedup_vs_plain": plain_ms / sur_ms,
+            "reject_rate": float(np.mean(rej)) / n,
+            "max_abs_dT_K": float(dT.max()), "max_abs_dT_accepted_K": float(dT[acc].max()) if
+            bool(acc.any()) else 0.0,
+            "linf_dY": float(dY.max()),
+            "max_element_rel_err_accepted": float(rel[:, acc].max()) if bool(acc.any()) else 0.0,
+            "network": "13 -> 3 x 256 GELU -> 10, BF16 tcgen05 / FP32 accumulate",
+            "train_samples": n_train, "train_epochs": args.sur_epochs, "batch": 8192,
+            "final_loss": losses[-1] if losses else None,
+            "sample_gen_s": t_gen, "train_s": t_train,
+            "judge": "FP64 GPU integrator on the same cells (atol 1e-11, rtol 1e-4)"}
 
 
 def run_reference(args, ws, rank):
@@ -422,6 +510,10 @@ def main():
     ap.add_argument("--block", type=int, default=64)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--surrogate", type=int, default=1,
+                    help="1: also train and time the gated surrogate (batched workload)")
+    ap.add_argument("--sur-samples", type=int, default=4194304)
+    ap.add_argument("--sur-epochs", type=int, default=4)
     args = ap.parse_args()
     if args.warmup < 1:
         raise SystemExit("--warmup must be >= 1")

@@ -305,24 +305,28 @@ struct CellCtx {
         double dqjdT = dkfdT - dkrdT;
         double dgdT = 0.0;
         double kind = 0.0;
+        // third-body and fall-off columns are rank one in the efficiencies:
+        // d q / d c_i = eff_i * g_r, with g_r = q / M (third body) or
+        // q (k0/kinf) (1/(Pr(1+Pr)) + F'/(Pr F)) (fall-off,
+        // unimolecularFallOffRR::gamDGamDCi, unimolecularFallOffRR.cpp:55-91);
+        // the record carries g_r so that each row adds eff_i * (coef g_r)
         if (type == kThirdBody) {
             kind = 1.0;
-            rec[11] = hmax(M, kTiny);
+            rec[11] = q / hmax(M, kTiny);
         } else if (type != kArrhenius) {
             if (M > kTiny) {
-                // unimolecularFallOffRR::gamDGamDCi / gamDGamDT (unimolecularFallOffRR.cpp:55-91)
+                // unimolecularFallOffRR::gamDGamDT (unimolecularFallOffRR.cpp:55-91)
                 const double Pr2 = k0 * M / notZeroD(kinf);
                 const double F2 = fall_F(type, lf, Pr2);
                 const double dPrdT = Pr2 * ((k0 * invT * (b0 + Ta0 * invT)) / notZeroD(k0) -
                                             (kinf * invT * (b + Ta * invT)) / notZeroD(kinf));
                 const double dFdT = troe_dfdt(type, &m.troe[4 * r], T, Pr2, F2, dPrdT);
                 dgdT = q * (dPrdT / (Pr2 * (1 + Pr2)) + dFdT / F2);
-                kind = 2.0;
-                rec[11] = k0;
-                rec[12] = kinf;
-                rec[13] = Pr2;
-                rec[14] = F2;
-                rec[15] = troe_dfdci_factor(type, lf, Pr2, F2);
+                const double fabc = troe_dfdci_factor(type, lf, Pr2, F2);
+                const double g = q * (k0 / notZeroD(kinf)) *
+                                 (1.0 / (Pr2 * (1 + Pr2)) + fabc * (1.0 / Pr2) / F2);
+                kind = finite(g) ? 2.0 : 3.0;
+                rec[11] = g;
             } else {
                 kind = 3.0;
             }
@@ -343,22 +347,10 @@ struct CellCtx {
         for (int k = 0; k < nf; ++k) Jrow[ldg(&m.fidx[kMaxSide * r + k])] += coef * rec[2 + k];
         for (int k = 0; k < nb; ++k) Jrow[ldg(&m.bidx[kMaxSide * r + k])] += (-coef) * rec[6 + k];
         const double kind = rec[10];
-        if (kind == 1.0) {
+        if (kind == 1.0 || kind == 2.0) {
             const double *e = &m.eff[(int64_t)r * nsp];
-            const double Mm = rec[11];
-            for (int i = 0; i < nsp; ++i) {
-                const double gg = ldg(&e[i]) / Mm;
-                if (finite(gg)) Jrow[i] += (coef * gg) * q;
-            }
-        } else if (kind == 2.0) {
-            const double *e = &m.eff[(int64_t)r * nsp];
-            const double k0 = rec[11], kinf = rec[12], Pr = rec[13], F = rec[14], fabc = rec[15];
-            for (int i = 0; i < nsp; ++i) {
-                const double dPrdci = ldg(&e[i]) * k0 / notZeroD(kinf);
-                const double dFdci = fabc * (1.0 / (Pr)*dPrdci);
-                const double gg = (dPrdci / (Pr * (1 + Pr)) + dFdci / F);
-                if (finite(gg)) Jrow[i] += (coef * gg) * q;
-            }
+            const double s = coef * rec[11];
+            for (int i = 0; i < nsp; ++i) Jrow[i] += ldg(&e[i]) * s;
         }
         Jrow[nsp] += coef * rec[1];
     }

@@ -114,3 +114,166 @@ def gemm_bf16(A: torch.Tensor, B: torch.Tensor, bias: Optional[torch.Tensor] = N
                                              _vp(bias), act, _vp(Cm), _vp_stream()),
                 "hc_gemm_bf16_tn")
     return Cm
+
+
+def element_projector(tables) -> np.ndarray:
+    """P = I - A^T (A A^T)^+ A with A[e][i] = atoms of element e in species i
+    / W_i: P dY conserves every element's mass (and so sum dY = 0)."""
+    A = tables.elem_matrix / tables.W[None, :]
+    A = A[np.abs(A).sum(axis=1) > 0]
+    nsp = tables.nsp
+    P = np.eye(nsp) - A.T @ np.linalg.pinv(A @ A.T) @ A
+    return np.ascontiguousarray(P)
+
+
+class Surrogate:
+    """Gated learned chemistry step for one mechanism.
+
+    The network predicts the normalised increment (dT, dY) of a flow step
+    from the normalised (T, ln p, Y, ln dt); the FP64 gate
+    (hc_surrogate_gate) projects dY onto element conservation, recovers T
+    from the conserved enthalpy and accepts or rejects each cell; rejected
+    cells are integrated by the FP64 integrator (hc_integrate_subset)."""
+
+    def __init__(self, mech, n_hidden: int = 3, width: int = 256, max_batch: int = 65536,
+                 seed: int = 0):
+        self.mech = mech
+        t = mech.tables
+        self.nsp = t.nsp
+        self.n_in, self.n_out = t.nsp + 3, t.nsp + 1
+        self.net = MLP(self.n_in, self.n_out, n_hidden, width, max_batch=max_batch, seed=seed)
+        dev = torch.device("cuda", torch.cuda.current_device())
+        self.dev = dev
+        self.proj = torch.tensor(element_projector(t), dtype=torch.float64, device=dev)
+        self.in_mean = torch.zeros(self.n_in, dtype=torch.float64, device=dev)
+        self.in_istd = torch.ones(self.n_in, dtype=torch.float64, device=dev)
+        self.out_mean = torch.zeros(self.n_out, dtype=torch.float64, device=dev)
+        self.out_std = torch.ones(self.n_out, dtype=torch.float64, device=dev)
+        self.gate = _capi.HcGateOpts(tol_T=2.0, tol_proj=0.5, y_neg=1e-12, x_max=8.0, T_min=250.0,
+                                     T_max=4000.0)
+
+    # ------------------------------------------------------------------ data
+    def features(self, T, p, Y, dt, dt_factor: float = 1.0, out=None) -> torch.Tensor:
+        n = int(T.shape[0])
+        X = out if out is not None else torch.empty((n, self.n_in), dtype=torch.float32,
+                                                    device=T.device)
+        _capi.check(_capi.load().hc_surrogate_features(
+            self.mech.handle, n, _vp(T), _vp(p), _vp(Y), _vp(dt), float(dt_factor),
+            _vp(self.in_mean), _vp(self.in_istd), _vp(X), _vp_stream()),
+            "hc_surrogate_features")
+        return X
+
+    @staticmethod
+    def raw_features(T, p, Y, dt):
+        return torch.cat([T[None], torch.log(p)[None], Y, torch.log(dt)[None]], dim=0).T
+
+    def fit_normalisation(self, T, p, Y, dt, dT, dY):
+        """Input / output statistics of the training set (float64)."""
+        raw = self.raw_features(T, p, Y, dt)
+        mu, sd = raw.mean(0), raw.std(0)
+        self.in_mean = mu.contiguous()
+        self.in_istd = torch.where(sd > 1e-12, 1.0 / sd, torch.ones_like(sd)).contiguous()
+        d = torch.cat([dT[None], dY], dim=0).T
+        self.out_mean = d.mean(0).contiguous()
+        osd = d.std(0)
+        self.out_std = torch.where(osd > 1e-30, osd, torch.ones_like(osd)).contiguous()
+
+    def targets(self, dT, dY) -> torch.Tensor:
+        d = torch.cat([dT[None], dY], dim=0).T
+        return ((d - self.out_mean) / self.out_std).to(torch.float32).contiguous()
+
+    # ------------------------------------------------------------------ train
+    def train(self, X: torch.Tensor, D: torch.Tensor, epochs: int = 4, batch: int = 8192,
+              lr: float = 2e-3, lr_final: float = 5e-5, seed: int = 0, log=None):
+        """Adam over shuffled mini-batches with a cosine learning-rate decay."""
+        n = int(X.shape[0])
+        steps_per_epoch = max(1, n // batch)
+        total = epochs * steps_per_epoch
+        g = torch.Generator(device=X.device).manual_seed(seed)
+        k = 0
+        losses = []
+        for ep in range(epochs):
+            perm = torch.randperm(n, device=X.device, generator=g)
+            for s in range(steps_per_epoch):
+                idx = perm[s * batch:(s + 1) * batch]
+                xb, yb = X[idx].contiguous(), D[idx].contiguous()
+                a = lr_final + 0.5 * (lr - lr_final) * (1 + np.cos(np.pi * k / max(1, total)))
+                want = (s == steps_per_epoch - 1)
+                l = self.net.train_step(xb, yb, a, want_loss=want, check=want)
+                if want:
+                    losses.append(l)
+                    if log:
+                        log(f"epoch {ep} loss {l:.4e}")
+                k += 1
+        return losses
+
+    # ------------------------------------------------------------------ infer
+    def step(self, flow, dt: torch.Tensor, dt_factor: float = 1.0, opts=None,
+             subdt: Optional[torch.Tensor] = None):
+        """One gated surrogate flow step on `flow` (T, p, rho, Y updated in
+        place). Returns (n_rejected, accept mask)."""
+        n = flow.n
+        X = self.features(flow.T, flow.p, flow.Y, dt, dt_factor)
+        pred = self.net.forward(X)
+        accept = torch.empty(n, dtype=torch.int32, device=flow.T.device)
+        rejected = torch.empty(n, dtype=torch.int32, device=flow.T.device)
+        nrej = C.c_int64(0)
+        _capi.check(_capi.load().hc_surrogate_gate(
+            self.mech.handle, n, _vp(flow.T), _vp(flow.p), _vp(flow.rho), _vp(flow.Y), _vp(pred),
+            _vp(X), _vp(self.out_mean), _vp(self.out_std), _vp(self.proj), C.byref(self.gate),
+            _vp(accept), _vp(rejected), C.byref(nrej), _vp_stream()), "hc_surrogate_gate")
+        nr = int(nrej.value)
+        if nr > 0:
+            o = opts if opts is not None else _capi.default_opts()
+            sub = subdt if subdt is not None else (dt * dt_factor).clone()
+            _capi.check(_capi.load().hc_integrate_subset(
+                self.mech.handle, C.byref(o), n, nr, _vp(rejected), _vp(flow.T), _vp(flow.p),
+                _vp(flow.rho), _vp(flow.Y), _vp(dt), float(dt_factor), _vp(sub), None, None, None,
+                None, _vp_stream()), "hc_integrate_subset")
+        return nr, accept
+
+
+def integrate_device(mech, T, p, rho, Y, dt, opts=None):
+    """FP64 integration of device arrays over per-cell dt (in place);
+    returns the per-cell status."""
+    n = int(T.shape[0])
+    o = opts if opts is not None else _capi.default_opts()
+    sub = dt.clone()
+    status = torch.zeros(n, dtype=torch.int32, device=T.device)
+    _capi.check(_capi.load().hc_integrate(mech.handle, C.byref(o), n, _vp(T), _vp(p), _vp(rho),
+                                          _vp(Y), _vp(dt), 1.0, _vp(sub), None, _vp(status), None,
+                                          _vp_stream()), "hc_integrate")
+    return status
+
+
+def generate_samples(mech, T, p, rho, Y, dt_nominal: float, n_samples: int, seed: int = 0,
+                     t_max: float = 3e-4, dt_spread: float = 3.0, opts=None):
+    """Training samples for the surrogate from the FP64 GPU integrator.
+
+    Starting states (T, p, rho, Y: device arrays of base cells) are tiled to
+    n_samples, advanced along their own reaction trajectories by a random
+    time in [0, t_max] (so that states part-way through ignition appear), and
+    then integrated over a flow step dt drawn log-uniformly in
+    [dt_nominal / dt_spread, dt_nominal * dt_spread]. Returns the
+    pre-step state, dt and the increments (dT, dY)."""
+    dev = T.device
+    g = torch.Generator(device=dev).manual_seed(seed)
+    nb = int(T.shape[0])
+    idx = torch.randint(0, nb, (n_samples,), device=dev, generator=g)
+    T1, p1, r1 = T[idx].contiguous(), p[idx].contiguous(), rho[idx].contiguous()
+    Y1 = Y[:, idx].contiguous()
+    tau = torch.rand(n_samples, device=dev, dtype=torch.float64, generator=g) * t_max
+    tau = torch.where(tau < 1e-9, torch.full_like(tau, 1e-9), tau)
+    # half of the samples stay at their drawn state (tau tiny), half move along
+    keep = torch.rand(n_samples, device=dev, generator=g) < 0.5
+    tau = torch.where(keep, torch.full_like(tau, 1e-12), tau)
+    integrate_device(mech, T1, p1, r1, Y1, tau, opts)
+    u = torch.rand(n_samples, device=dev, dtype=torch.float64, generator=g)
+    dt = dt_nominal * torch.exp((2.0 * u - 1.0) * np.log(dt_spread))
+    T2, r2, Y2 = T1.clone(), r1.clone(), Y1.clone()
+    st = integrate_device(mech, T2, p1, r2, Y2, dt, opts)
+    good = (st & 12) == 0
+    sel = torch.nonzero(good).flatten()
+    return {"T": T1[sel].contiguous(), "p": p1[sel].contiguous(), "rho": r1[sel].contiguous(),
+            "Y": Y1[:, sel].contiguous(), "dt": dt[sel].contiguous(),
+            "dT": (T2 - T1)[sel].contiguous(), "dY": (Y2 - Y1)[:, sel].contiguous()}

@@ -29,7 +29,8 @@ def test_gemm_bf16_matches_fp32_product(M, N, K):
     out = gemm_bf16(A, B, bias)
     torch.cuda.synchronize()
     err = (out - ref).abs().max().item() / ref.abs().max().item()
-    assert err < 1e-5, err        # same bf16 operands, fp32 accumulation: order only
+    # same bf16 operands, fp32 accumulation: only the summation order differs
+    assert err < 1e-5 * max(1.0, (K / 512) ** 0.5), err
     ref_g = torch.nn.functional.gelu(ref)
     out_g = gemm_bf16(A, B, bias, act=1)
     assert (out_g - ref_g).abs().max().item() < 1e-4 * ref.abs().max().item() + 1e-5
