@@ -136,13 +136,26 @@ const char *hc_last_error(void);
 void hc_default_opts(hc_opts *opts);
 
 /*
- * Kernel selection for hc_integrate*: kernel 0 = automatic (thread per cell
- * when nsp + 1 <= 16, else a cell group of 32/64 lanes), 1 = thread per cell,
- * 2 = cell group; block = threads per block of the thread-per-cell kernel
- * (32, 64 or 128). Set by the autotuner (openhurricane_b200/autotune.py). No
- * reference counterpart.
+ * Kernel selection for hc_integrate*: kernel 0 = automatic (the compact
+ * thread-per-cell kernel when nsp + 1 <= 16 and the mechanism fits its
+ * tables, else the table-driven thread-per-cell kernel; a cell group of 32/64
+ * lanes above 16 unknowns), 1 = table-driven thread per cell, 2 = cell group,
+ * 3 = thread per cell generated for this mechanism (every index and
+ * coefficient a literal; compiled with NVRTC for sm_100a on first use, which
+ * must precede any stream capture), 4 = compact thread per cell (mechanism
+ * in the kernel's constant parameter bank: nsp <= 15, <= 64 reactions);
+ * block = threads per block of the thread-per-cell kernels (32, 64 or 128). Set by the autotuner (openhurricane_b200/autotune.py).
+ * No reference counterpart.
  */
 int hc_set_tuning(hc_mech_t mech, int kernel, int block);
+
+/* The generated kernel's CUDA source for a mechanism (len = its length; up to
+ * cap-1 bytes and a terminating 0 are written to buf when buf != NULL).
+ * Host-only: needs no GPU. */
+int hc_jit_source(const hc_mech_desc *desc, int block, char *buf, int64_t cap, int64_t *len);
+/* Compile that source with NVRTC for sm_100a without loading it (host only);
+ * cubin_bytes receives the size of the compiled image. */
+int hc_jit_compile(const hc_mech_desc *desc, int block, int64_t *cubin_bytes);
 
 /* Upload a mechanism; selects the compiled kernel variant for nsp. */
 int hc_mech_create(const hc_mech_desc *desc, hc_mech_t *out);

@@ -2,6 +2,8 @@
 
 Candidates are (kernel, block) pairs accepted by hc_set_tuning:
 kernel 1 = thread per cell (nsp + 1 <= 16; block 32/64/128 threads),
+kernel 3 = thread per cell generated for the mechanism (same limits),
+kernel 4 = compact thread per cell (mechanism in the constant bank),
 kernel 2 = cell group (32 lanes per cell up to 32 unknowns, 64 above; the
 block argument is ignored).
 Each candidate integrates the same sample of cells (a strided subset of the
@@ -28,7 +30,7 @@ _MEMO: Dict[str, dict] = {}
 def candidates(nsp: int) -> List[Tuple[int, int]]:
     c = []
     if nsp + 1 <= 16:
-        c += [(1, 32), (1, 64), (1, 128)]
+        c += [(4, 32), (4, 64), (4, 128), (3, 64), (1, 64)]
     c += [(2, 64)]      # the cell group's width is fixed by the variant; block is unused
     return c
 

@@ -17,6 +17,8 @@
 #include <vector>
 
 #include "../../include/hurchem_b200.h"
+#include "integrator_t2.cuh"
+#include "jit.h"
 #include "surrogate.cuh"
 #include "variants.h"
 
@@ -80,9 +82,18 @@ struct hc_mech_s {
     // states (ImplicitEuler's yklast_), grown on demand
     double *ylast = nullptr;
     size_t ylast_cells = 0;
-    // kernel choice (hc_set_tuning): 0 automatic, 1 thread per cell, 2 cell group
+    // kernel choice (hc_set_tuning): 0 automatic, 1 thread per cell, 2 cell
+    // group, 3 mechanism-specialised thread per cell (generated, NVRTC)
     int kernel = 0;
     int block = 64;
+    // host tables in device order, for the generated kernels
+    HostMech host;
+    // the mechanism in the compact thread-per-cell kernel's parameter form
+    T2Mech t2{};
+    bool t2_ok = false;
+    JitKernel jit;
+    bool jit_tried = false;
+    std::string jit_err;
 };
 
 namespace {
@@ -142,6 +153,126 @@ int check_opts(const hc_opts *o) {
 
 }  // namespace
 
+// Host copy of the tables in device order. Reactions are regrouped by rate
+// law (plain Arrhenius, third-body, fall-off), stable within a group, so that
+// the lanes of a cell group evaluating one chunk of reactions mostly follow
+// the same code path. Source terms are sums over reactions; only their
+// summation order changes.
+static void make_host(const hc_mech_desc *d, HostMech &h) {
+    const int nsp = d->nsp, nrc = d->nrc;
+    std::vector<int> perm(nrc);
+    for (int r = 0; r < nrc; ++r) perm[r] = r;
+    auto cls = [&](int r) { return d->rate_type[r] >= HC_RATE_LINDEMANN ? 2 : d->rate_type[r]; };
+    std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return cls(a) < cls(b); });
+    auto permute = [&](const auto *src, int width) {
+        using V = std::remove_const_t<std::remove_pointer_t<decltype(src)>>;
+        std::vector<V> outv((size_t)nrc * width);
+        for (int r = 0; r < nrc; ++r)
+            for (int k = 0; k < width; ++k)
+                outv[(size_t)r * width + k] = src[(size_t)perm[r] * width + k];
+        return outv;
+    };
+    h.nsp = nsp;
+    h.nrc = nrc;
+    h.W.assign(d->W, d->W + nsp);
+    h.Trange.assign(d->Trange, d->Trange + 3 * (size_t)nsp);
+    h.nasa.assign(d->nasa, d->nasa + 14 * (size_t)nsp);
+    h.rate_type = permute(d->rate_type, 1);
+    h.reversible = permute(d->reversible, 1);
+    h.arr = permute(d->arr, 3);
+    h.arr0 = permute(d->arr0, 3);
+    h.troe = permute(d->troe, 4);
+    h.eff = permute(d->eff, nsp);
+    h.nf = permute(d->nf, 1);
+    h.nb = permute(d->nb, 1);
+    h.fidx = permute(d->fidx, HC_MAX_SIDE);
+    h.bidx = permute(d->bidx, HC_MAX_SIDE);
+    h.fnu = permute(d->fnu, HC_MAX_SIDE);
+    h.bnu = permute(d->bnu, HC_MAX_SIDE);
+    h.ford = permute(d->ford, HC_MAX_SIDE);
+    h.bord = permute(d->bord, HC_MAX_SIDE);
+    h.sum_stoi.assign(nrc, 0.0);
+    for (int r = 0; r < nrc; ++r) {
+        double s = 0.0;
+        for (int k = 0; k < h.nf[r]; ++k) s -= h.fnu[HC_MAX_SIDE * r + k];
+        for (int k = 0; k < h.nb[r]; ++k) s += h.bnu[HC_MAX_SIDE * r + k];
+        h.sum_stoi[r] = s;
+    }
+}
+
+// the mechanism in T2Mech form, if it fits the compact kernel's tables
+static bool pack_t2(const HostMech &h, const hc_mech_desc *d, T2Mech &t) {
+    if (h.nsp > kT2MaxSp || h.nrc > kT2MaxRxn) return false;
+    std::memset(&t, 0, sizeof(t));
+    t.nsp = h.nsp;
+    t.nrc = h.nrc;
+    for (int i = 0; i < h.nsp; ++i) {
+        t.W[i] = h.W[i];
+        for (int k = 0; k < 3; ++k) t.thermo[i][k] = h.Trange[3 * i + k];
+        for (int k = 0; k < 14; ++k) t.thermo[i][3 + k] = h.nasa[14 * i + k];
+    }
+    int ne = 0;
+    for (int r = 0; r < h.nrc; ++r) {
+        T2Rxn &R = t.rxn[r];
+        R.A = h.arr[3 * r];
+        R.b = h.arr[3 * r + 1];
+        R.Ta = h.arr[3 * r + 2];
+        R.A0 = h.arr0[3 * r];
+        R.b0 = h.arr0[3 * r + 1];
+        R.Ta0 = h.arr0[3 * r + 2];
+        for (int k = 0; k < 4; ++k) R.troe[k] = h.troe[4 * r + k];
+        for (int k = 0; k < HC_MAX_SIDE; ++k) {
+            R.fnu[k] = h.fnu[HC_MAX_SIDE * r + k];
+            R.bnu[k] = h.bnu[HC_MAX_SIDE * r + k];
+            R.ford[k] = h.ford[HC_MAX_SIDE * r + k];
+            R.bord[k] = h.bord[HC_MAX_SIDE * r + k];
+            R.fidx[k] = (int8_t)h.fidx[HC_MAX_SIDE * r + k];
+            R.bidx[k] = (int8_t)h.bidx[HC_MAX_SIDE * r + k];
+        }
+        R.sum_stoi = h.sum_stoi[r];
+        R.type = (int8_t)h.rate_type[r];
+        R.rev = (int8_t)(h.reversible[r] != 0);
+        R.nf = (int8_t)h.nf[r];
+        R.nb = (int8_t)h.nb[r];
+        R.eff_begin = (int16_t)ne;
+        if (h.rate_type[r] != HC_RATE_ARRHENIUS) {
+            for (int i = 0; i < h.nsp; ++i) {
+                const double e = h.eff[(size_t)r * h.nsp + i];
+                if (e == 0.0) continue;
+                if (ne >= kT2MaxEff) return false;
+                t.eff_val[ne] = e;
+                t.eff_idx[ne] = (int8_t)i;
+                ++ne;
+            }
+        }
+        R.eff_end = (int16_t)ne;
+    }
+    (void)d;
+    return true;
+}
+
+static int check_desc(const hc_mech_desc *d) {
+    const int nsp = d->nsp, nrc = d->nrc;
+    if (nsp < 1 || nrc < 0) return fail(HC_E_INVALID, "bad mechanism size");
+    if (!d->W || !d->Trange || !d->nasa || (nrc > 0 && (!d->rate_type || !d->reversible ||
+        !d->arr || !d->arr0 || !d->troe || !d->eff || !d->nf || !d->nb || !d->fidx ||
+        !d->bidx || !d->fnu || !d->bnu || !d->ford || !d->bord)))
+        return fail(HC_E_INVALID, "null table in mechanism");
+    for (int r = 0; r < nrc; ++r) {
+        if (d->nf[r] < 0 || d->nf[r] > HC_MAX_SIDE || d->nb[r] < 0 || d->nb[r] > HC_MAX_SIDE)
+            return fail(HC_E_INVALID, "reaction side larger than HC_MAX_SIDE");
+        if (d->rate_type[r] < 0 || d->rate_type[r] > HC_RATE_TROE4)
+            return fail(HC_E_INVALID, "unknown rate type");
+        for (int k = 0; k < d->nf[r]; ++k)
+            if (d->fidx[HC_MAX_SIDE * r + k] < 0 || d->fidx[HC_MAX_SIDE * r + k] >= nsp)
+                return fail(HC_E_INVALID, "species index out of range");
+        for (int k = 0; k < d->nb[r]; ++k)
+            if (d->bidx[HC_MAX_SIDE * r + k] < 0 || d->bidx[HC_MAX_SIDE * r + k] >= nsp)
+                return fail(HC_E_INVALID, "species index out of range");
+    }
+    return HC_OK;
+}
+
 extern "C" {
 
 int hc_abi_version(void) { return HC_ABI_VERSION; }
@@ -174,64 +305,28 @@ int hc_mech_create(const hc_mech_desc *d, hc_mech_t *out) {
     if (!d || !out) return fail(HC_E_INVALID, "null argument");
     *out = nullptr;
     const int nsp = d->nsp, nrc = d->nrc;
-    if (nsp < 1 || nrc < 0) return fail(HC_E_INVALID, "bad mechanism size");
+    {
+        const int vrc = check_desc(d);
+        if (vrc != HC_OK) return vrc;
+    }
     const int variant = variant_for(nsp + 1);
     if (variant < 0)
         return fail(HC_E_UNSUPPORTED, "mechanisms with more than 63 species are not built");
-    if (!d->W || !d->Trange || !d->nasa || (nrc > 0 && (!d->rate_type || !d->reversible ||
-        !d->arr || !d->arr0 || !d->troe || !d->eff || !d->nf || !d->nb || !d->fidx ||
-        !d->bidx || !d->fnu || !d->bnu || !d->ford || !d->bord)))
-        return fail(HC_E_INVALID, "null table in mechanism");
-    for (int r = 0; r < nrc; ++r) {
-        if (d->nf[r] < 0 || d->nf[r] > HC_MAX_SIDE || d->nb[r] < 0 || d->nb[r] > HC_MAX_SIDE)
-            return fail(HC_E_INVALID, "reaction side larger than HC_MAX_SIDE");
-        if (d->rate_type[r] < 0 || d->rate_type[r] > HC_RATE_TROE4)
-            return fail(HC_E_INVALID, "unknown rate type");
-        for (int k = 0; k < d->nf[r]; ++k)
-            if (d->fidx[HC_MAX_SIDE * r + k] < 0 || d->fidx[HC_MAX_SIDE * r + k] >= nsp)
-                return fail(HC_E_INVALID, "species index out of range");
-        for (int k = 0; k < d->nb[r]; ++k)
-            if (d->bidx[HC_MAX_SIDE * r + k] < 0 || d->bidx[HC_MAX_SIDE * r + k] >= nsp)
-                return fail(HC_E_INVALID, "species index out of range");
-    }
-    // Reactions are regrouped by rate law (plain Arrhenius, third-body,
-    // fall-off), stable within a group, so that the lanes of a cell group
-    // evaluating one chunk of reactions mostly follow the same code path.
-    // Source terms are sums over reactions; only their summation order changes.
-    std::vector<int> perm(nrc);
-    for (int r = 0; r < nrc; ++r) perm[r] = r;
-    auto cls = [&](int r) { return d->rate_type[r] >= HC_RATE_LINDEMANN ? 2 : d->rate_type[r]; };
-    std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return cls(a) < cls(b); });
-    auto permute = [&](const auto *src, int width) {
-        using V = std::remove_const_t<std::remove_pointer_t<decltype(src)>>;
-        std::vector<V> outv((size_t)nrc * width);
-        for (int r = 0; r < nrc; ++r)
-            for (int k = 0; k < width; ++k)
-                outv[(size_t)r * width + k] = src[(size_t)perm[r] * width + k];
-        return outv;
-    };
-    const auto p_type = permute(d->rate_type, 1), p_rev = permute(d->reversible, 1);
-    const auto p_arr = permute(d->arr, 3), p_arr0 = permute(d->arr0, 3), p_troe = permute(d->troe, 4);
-    const auto p_eff = permute(d->eff, nsp);
-    const auto p_nf = permute(d->nf, 1), p_nb = permute(d->nb, 1);
-    const auto p_fidx = permute(d->fidx, HC_MAX_SIDE), p_bidx = permute(d->bidx, HC_MAX_SIDE);
-    const auto p_fnu = permute(d->fnu, HC_MAX_SIDE), p_bnu = permute(d->bnu, HC_MAX_SIDE);
-    const auto p_ford = permute(d->ford, HC_MAX_SIDE), p_bord = permute(d->bord, HC_MAX_SIDE);
+    HostMech hm;
+    make_host(d, hm);
+    const auto &p_type = hm.rate_type, &p_rev = hm.reversible;
+    const auto &p_arr = hm.arr, &p_arr0 = hm.arr0, &p_troe = hm.troe, &p_eff = hm.eff;
+    const auto &p_nf = hm.nf, &p_nb = hm.nb, &p_fidx = hm.fidx, &p_bidx = hm.bidx;
+    const auto &p_fnu = hm.fnu, &p_bnu = hm.bnu, &p_ford = hm.ford, &p_bord = hm.bord;
     // participation lists per species, in (regrouped) reaction order:
     // coef = -nu' (reactant) / +nu'' (product)
     std::vector<std::vector<std::pair<int, double>>> part(nsp);
-    std::vector<double> sum_stoi(nrc);
+    const std::vector<double> &sum_stoi = hm.sum_stoi;
     for (int r = 0; r < nrc; ++r) {
-        double s = 0.0;
-        for (int k = 0; k < p_nf[r]; ++k) {
+        for (int k = 0; k < p_nf[r]; ++k)
             part[p_fidx[HC_MAX_SIDE * r + k]].push_back({r, -p_fnu[HC_MAX_SIDE * r + k]});
-            s -= p_fnu[HC_MAX_SIDE * r + k];
-        }
-        for (int k = 0; k < p_nb[r]; ++k) {
+        for (int k = 0; k < p_nb[r]; ++k)
             part[p_bidx[HC_MAX_SIDE * r + k]].push_back({r, p_bnu[HC_MAX_SIDE * r + k]});
-            s += p_bnu[HC_MAX_SIDE * r + k];
-        }
-        sum_stoi[r] = s;
     }
     std::vector<int32_t> sp_ptr(nsp + 1, 0), sp_rxn;
     std::vector<double> sp_coef;
@@ -246,6 +341,8 @@ int hc_mech_create(const hc_mech_desc *d, hc_mech_t *out) {
 
     hc_mech_s *m = new hc_mech_s();
     m->variant = variant;
+    m->host = hm;
+    m->t2_ok = pack_t2(hm, d, m->t2);
     DevMech &dm = m->dm;
     dm.nsp = nsp;
     dm.nrc = nrc;
@@ -327,11 +424,49 @@ int hc_mech_create(const hc_mech_desc *d, hc_mech_t *out) {
 
 int hc_set_tuning(hc_mech_t m, int kernel, int block) {
     if (!m) return fail(HC_E_INVALID, "null mechanism");
-    if (kernel < 0 || kernel > 2) return fail(HC_E_INVALID, "kernel must be 0, 1 or 2");
+    if (kernel < 0 || kernel > 4) return fail(HC_E_INVALID, "kernel must be 0 .. 4");
     if (block != 32 && block != 64 && block != 128)
         return fail(HC_E_INVALID, "block must be 32, 64 or 128");
+    if (block != m->block) {
+        m->jit_tried = false;   // the generated kernel is built per block size
+        m->jit = JitKernel();
+    }
     m->kernel = kernel;
     m->block = block;
+    return HC_OK;
+}
+
+int hc_jit_compile(const hc_mech_desc *d, int block, int64_t *cubin_bytes) {
+    if (!d || !cubin_bytes) return fail(HC_E_INVALID, "null argument");
+    int64_t len = 0;
+    int rc = hc_jit_source(d, block, nullptr, 0, &len);
+    if (rc != HC_OK) return rc;
+    HostMech h;
+    make_host(d, h);
+    std::vector<char> cubin;
+    std::string err;
+    rc = jit_compile(jit_t1_source(h, block), cubin, err);
+    if (rc != HC_OK) return fail(rc, err);
+    *cubin_bytes = (int64_t)cubin.size();
+    return HC_OK;
+}
+
+int hc_jit_source(const hc_mech_desc *d, int block, char *buf, int64_t cap, int64_t *len) {
+    if (!d || !len) return fail(HC_E_INVALID, "null argument");
+    const int vrc = check_desc(d);
+    if (vrc != HC_OK) return vrc;
+    if (d->nsp + 1 > 16) return fail(HC_E_UNSUPPORTED, "no generated kernel for nsp + 1 > 16");
+    if (block != 32 && block != 64 && block != 128)
+        return fail(HC_E_INVALID, "block must be 32, 64 or 128");
+    HostMech h;
+    make_host(d, h);
+    const std::string src = jit_t1_source(h, block);
+    *len = (int64_t)src.size();
+    if (buf && cap > 0) {
+        const size_t n = std::min<size_t>((size_t)cap - 1, src.size());
+        std::memcpy(buf, src.data(), n);
+        buf[n] = 0;
+    }
     return HC_OK;
 }
 
@@ -387,7 +522,42 @@ static int integrate_impl(hc_mech_t m, const hc_opts *opts, int64_t ncells, doub
     if (m->kernel == 1 && !t1_ok)
         return fail(HC_E_UNSUPPORTED,
                     "thread-per-cell kernel needs nsp <= 15 and autoUpdateJacobian off");
-    const bool use_t1 = t1_ok && (m->kernel == 0 || m->kernel == 1);
+    if (m->kernel == 4 && !(t1_ok && m->t2_ok))
+        return fail(HC_E_UNSUPPORTED,
+                    "compact thread-per-cell kernel needs nsp <= 15, <= 64 reactions and "
+                    "autoUpdateJacobian off");
+    const bool use_t2 = t1_ok && m->t2_ok && (m->kernel == 4 || m->kernel == 0);
+    if (use_t2) {
+        if (m->ylast_cells < (size_t)ncells) {
+            // grows only: a first call with a new, larger size synchronises the
+            // stream and must therefore come before any stream capture
+            HC_CUDA(cudaStreamSynchronize(st));
+            if (m->ylast) HC_CUDA(cudaFree(m->ylast));
+            m->ylast = nullptr;
+            m->ylast_cells = 0;
+            HC_CUDA(cudaMalloc(&m->ylast, sizeof(double) * 2 * 16 * (size_t)ncells));
+            m->ylast_cells = (size_t)ncells;
+        }
+        return variant_integrate_t2(N, m->t2, m->num_sms, P, io, m->ylast, m->block, st, g_err);
+    }
+    if (m->kernel == 3 && !t1_ok)
+        return fail(HC_E_UNSUPPORTED,
+                    "generated thread-per-cell kernel needs nsp <= 15 and autoUpdateJacobian off");
+    bool use_jit = t1_ok && m->kernel == 3;
+    if (use_jit && !m->jit_tried) {
+        // first use: generate, compile and load (host work, no stream operation)
+        m->jit_tried = true;
+        std::string err;
+        if (jit_build_t1(m->host, m->block, &m->jit, err) != HC_OK) {
+            m->jit = JitKernel();
+            m->jit_err = err;
+        }
+    }
+    if (use_jit && !m->jit.func) {
+        if (m->kernel == 3) return fail(HC_E_UNSUPPORTED, "generated kernel unavailable: " + m->jit_err);
+        use_jit = false;   // automatic choice: the precompiled thread-per-cell kernel
+    }
+    const bool use_t1 = t1_ok && (m->kernel == 0 || m->kernel == 1 || use_jit);
     if (use_t1) {
         if (m->ylast_cells < (size_t)ncells) {
             // grows only: a first call with a new, larger size synchronises the
@@ -399,6 +569,7 @@ static int integrate_impl(hc_mech_t m, const hc_opts *opts, int64_t ncells, doub
             HC_CUDA(cudaMalloc(&m->ylast, sizeof(double) * 2 * 16 * (size_t)ncells));
             m->ylast_cells = (size_t)ncells;
         }
+        if (use_jit) return jit_launch_t1(m->jit, m->num_sms, P, io, m->ylast, st, g_err);
         return variant_integrate_t1(N, m->dm, m->num_sms, P, io, m->ylast, m->block, st, g_err);
     }
     HC_DISPATCH(m, integrate, m->dm, m->num_sms, P, io, st, g_err);

@@ -1,6 +1,8 @@
-// Cooperative "cell group": G lanes (one warp for G = 32, two warps for
-// G = 64) that integrate one cell together, lane i owning row i of the
-// Newton matrix and element i of every state vector.
+// Cooperative "cell group": G lanes (half a warp for G = 16, one warp for
+// G = 32, two warps for G = 64) that integrate one cell together, lane i
+// owning row i of the Newton matrix and element i of every state vector.
+// Two 16-lane groups share a warp and run independently: their shuffles and
+// warp barriers use the group's half-warp mask.
 //
 // All reductions return bit-identical results in every lane of the group
 // (xor-butterfly within a warp; the two warp partials are combined in a
@@ -14,17 +16,20 @@ namespace hc {
 
 template <int G>
 struct Group {
-    static_assert(G == 32 || G == 64, "cell group is one or two warps");
+    static_assert(G == 16 || G == 32 || G == 64, "cell group is half a warp, one or two warps");
+    static constexpr int GW = G < 32 ? G : 32;   // lanes of the group within one warp
     int lane;    // 0 .. G-1
-    int wlane;   // lane within its warp
+    int wlane;   // lane within the group's part of its warp (0 .. GW-1)
     int warp;    // warp within the group
     int barid;   // named barrier (G == 64)
+    int base;    // first lane of the group within its warp (G == 16: 0 or 16)
+    unsigned mask;   // the group's lanes within its warp
     double *red; // [4] cross-warp scratch
     int *redi;   // [4]
 
     __device__ __forceinline__ void sync() const {
-        if (G == 32) {
-            __syncwarp();
+        if (G <= 32) {
+            __syncwarp(mask);
         } else {
             asm volatile("bar.sync %0, %1;" ::"r"(barid), "r"(64) : "memory");
         }
@@ -32,7 +37,7 @@ struct Group {
 
     __device__ __forceinline__ double sum(double v) const {
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        for (int o = GW / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
         if (G == 64) {
             if (wlane == 0) red[warp] = v;
             sync();
@@ -44,8 +49,8 @@ struct Group {
 
     __device__ __forceinline__ double max(double v) const {
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const double w = __shfl_xor_sync(0xffffffffu, v, o);
+        for (int o = GW / 2; o > 0; o >>= 1) {
+            const double w = __shfl_xor_sync(mask, v, o);
             v = (v < w) ? w : v;
         }
         if (G == 64) {
@@ -59,7 +64,7 @@ struct Group {
 
     __device__ __forceinline__ int min_int(int v) const {
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v = ::min(v, __shfl_xor_sync(0xffffffffu, v, o));
+        for (int o = GW / 2; o > 0; o >>= 1) v = ::min(v, __shfl_xor_sync(mask, v, o));
         if (G == 64) {
             if (wlane == 0) redi[warp] = v;
             sync();
@@ -73,9 +78,9 @@ struct Group {
     __device__ __forceinline__ int argmax(double v) const {
         int idx = lane;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const double w = __shfl_xor_sync(0xffffffffu, v, o);
-            const int j = __shfl_xor_sync(0xffffffffu, idx, o);
+        for (int o = GW / 2; o > 0; o >>= 1) {
+            const double w = __shfl_xor_sync(mask, v, o);
+            const int j = __shfl_xor_sync(mask, idx, o);
             if (w > v || (w == v && j < idx)) {
                 v = w;
                 idx = j;

@@ -40,35 +40,10 @@
 
 namespace hc {
 
-struct IntegratorParams {
-    int32_t maxstep;
-    int32_t auto_update_jacobian;
-    int32_t step_to_update_jac;
-    double atol, rtol, safescale, minscale, maxscale, alphainc;
-    double atol_inc, rtol_inc, T_threshold, T_alpha, T_beta, dt_max;
-    double err_accept_limit;     // pow(maxscale/safescale, -1/alphainc)
-    int64_t max_newton_total;
-};
-
-struct CellIO {
-    int64_t ncells;         // field length (stride of species fields)
-    int64_t nqueue;         // cells to integrate: queue entries 0..nqueue-1
-    double *T;
-    const double *p;
-    double *rho;
-    double *Y;              // [nsp][ncells]
-    const double *dt;
-    double dt_factor;
-    double *subdt;
-    double *Ri;             // optional [nsp][ncells]
-    int32_t *status;        // optional
-    const int32_t *order;   // optional queue order (cell indices)
-    int64_t *cost;          // optional per-cell Newton iteration count out
-    unsigned long long *queue_head;
-    unsigned long long *counters;  // [6] n_jac, n_rhs, n_lu, n_newton, n_steps, n_attempts
-};
-
 constexpr int kRec = 16;   // doubles per reaction record
+
+// cells integrated by one block of 128 threads (a cell group of G lanes each)
+__host__ __device__ constexpr int cells_per_block(int G) { return 128 / G; }
 
 template <int N, int G>
 struct Smem {
@@ -108,7 +83,7 @@ struct CellCtx {
     // f(y) and, if jac, the analytic Jacobian rows into shared memory.
     // y is this lane's element (lane < N). Returns this lane's f element.
     // chemistrySource::DyDt (chemistrySource.cpp:863-883) / ::jacobian (:967-1021)
-    __device__ __noinline__ double evaluate(double y, bool jac) {
+    __device__ __forceinline__ double evaluate(double y, bool jac) {
         using L = Smem<N, G>;
         const int lane = g.lane;
         if (jac) ++n_jac; else ++n_rhs;
@@ -182,7 +157,7 @@ struct CellCtx {
     }
 
     // one reaction: q and the derivative pieces (reactionTypes.cpp:263-352, 354-445, 843-876)
-    __device__ __noinline__ void reaction_record(int r, double T, double logT, const double *c,
+    __device__ __forceinline__ void reaction_record(int r, double T, double logT, const double *c,
                                                  bool jac, double *rec) {
         using L = Smem<N, G>;
         const int type = ldg(&m.rate_type[r]);
@@ -381,7 +356,7 @@ struct CellCtx {
         if constexpr (K + 1 < N) lu_step<K + 1>(a, act, mystep);
     }
 
-    __device__ __noinline__ int factor(double dt) {
+    __device__ __forceinline__ int factor(double dt) {
         using L = Smem<N, G>;
         const int lane = g.lane;
         double a[N];
@@ -404,31 +379,32 @@ struct CellCtx {
     }
 
     // solve (LU) x = b; b is this lane's element; returns x element
-    __device__ __noinline__ double solve(int mystep, double b) {
+    __device__ __forceinline__ double solve(int mystep, double b) {
         using L = Smem<N, G>;
         const int lane = g.lane;
         if (mystep >= 0) s[L::kB + mystep] = b;
         g.sync();
         if (g.warp == 0) {
-            constexpr int R = (N + 31) / 32;
+            constexpr int GW = Group<G>::GW;
+            constexpr int R = (N + GW - 1) / GW;
             const int wl = g.wlane;
             double z[R], acc[R];
 #pragma unroll
             for (int q = 0; q < R; ++q) {
-                const int i = wl + 32 * q;
+                const int i = wl + GW * q;
                 z[q] = (i < N) ? s[L::kB + i] : 0.0;
                 acc[q] = 0.0;
             }
             // forward: z_i = b_i - sum_{t<i} L(i,t) z_t (ascending t)
 #pragma unroll
             for (int t = 0; t < N; ++t) {
-                const int q_t = t / 32, l_t = t % 32;
+                const int q_t = t / GW, l_t = t % GW;
                 const double mine = z[q_t] - acc[q_t];
-                const double zt = __shfl_sync(0xffffffffu, mine, l_t);
+                const double zt = __shfl_sync(g.mask, mine, g.base + l_t);
                 if (wl == l_t) z[q_t] = zt;
 #pragma unroll
                 for (int q = 0; q < R; ++q) {
-                    const int i = wl + 32 * q;
+                    const int i = wl + GW * q;
                     if (i > t && i < N) acc[q] += s[L::kJ + i * L::LD + t] * zt;
                 }
             }
@@ -437,13 +413,13 @@ struct CellCtx {
             for (int q = 0; q < R; ++q) acc[q] = 0.0;
 #pragma unroll
             for (int t = N - 1; t >= 0; --t) {
-                const int q_t = t / 32, l_t = t % 32;
+                const int q_t = t / GW, l_t = t % GW;
                 const double mine = (z[q_t] - acc[q_t]) / s[L::kJ + t * L::LD + t];
-                const double xt = __shfl_sync(0xffffffffu, mine, l_t);
+                const double xt = __shfl_sync(g.mask, mine, g.base + l_t);
                 if (wl == 0) s[L::kX + t] = xt;
 #pragma unroll
                 for (int q = 0; q < R; ++q) {
-                    const int i = wl + 32 * q;
+                    const int i = wl + GW * q;
                     if (i < t) acc[q] += s[L::kJ + i * L::LD + t] * xt;
                 }
             }
@@ -666,8 +642,10 @@ template <int G>
 __device__ __forceinline__ Group<G> make_group(double *s, int gid, int red_off, int redi_off) {
     Group<G> g;
     g.lane = threadIdx.x % G;
-    g.wlane = threadIdx.x & 31;
+    g.wlane = (G < 32) ? g.lane : (threadIdx.x & 31);
     g.warp = g.lane >> 5;
+    g.base = (G < 32) ? ((threadIdx.x & 31) & ~(G - 1)) : 0;
+    g.mask = (G < 32) ? (((1u << G) - 1u) << g.base) : 0xffffffffu;
     g.barid = 1 + gid;
     g.red = s + red_off;
     g.redi = reinterpret_cast<int *>(s + redi_off);
@@ -678,7 +656,7 @@ __device__ __forceinline__ Group<G> make_group(double *s, int gid, int red_off, 
 __device__ const IntegratorParams kNoParams{};
 
 template <int N, int G>
-__global__ void __launch_bounds__(G * ((G == 64) ? 2 : 4), (G == 64) ? 3 : 4)
+__global__ void __launch_bounds__(128, (G == 64) ? 2 : 3)
 integrate_kernel(const __grid_constant__ DevMech m, const __grid_constant__ IntegratorParams P,
                  const __grid_constant__ CellIO io) {
     using L = Smem<N, G>;
@@ -760,12 +738,12 @@ integrate_kernel(const __grid_constant__ DevMech m, const __grid_constant__ Inte
 // f(y) and the analytic Jacobian at given states (chemistrySource::DyDt,
 // ::jacobian); one cell group per state.
 template <int N, int G>
-__global__ void __launch_bounds__(G * ((G == 64) ? 2 : 4))
+__global__ void __launch_bounds__(128)
 rhs_jac_kernel(const __grid_constant__ DevMech m, int64_t n, const double *c, const double *T,
                const double *p, double *dydt, double *J) {
     using L = Smem<N, G>;
     extern __shared__ double smem_all[];
-    constexpr int CPB = (G == 64) ? 2 : 4;
+    constexpr int CPB = cells_per_block(G);
     const int gid = threadIdx.x / G;
     double *s = smem_all + (size_t)gid * L::kSize;
     const int64_t k = (int64_t)blockIdx.x * CPB + gid;
@@ -788,12 +766,12 @@ rhs_jac_kernel(const __grid_constant__ DevMech m, int64_t n, const double *c, co
 // explicit source terms omega_i W_i (chemistrySource::calculateSourceTerms,
 // chemistrySource.cpp:1370-1406)
 template <int N, int G>
-__global__ void __launch_bounds__(G * ((G == 64) ? 2 : 4))
+__global__ void __launch_bounds__(128)
 source_kernel(const __grid_constant__ DevMech m, int64_t n, const double *T, const double *p,
               const double *rho, const double *Y, double *Ri) {
     using L = Smem<N, G>;
     extern __shared__ double smem_all[];
-    constexpr int CPB = (G == 64) ? 2 : 4;
+    constexpr int CPB = cells_per_block(G);
     const int gid = threadIdx.x / G;
     double *s = smem_all + (size_t)gid * L::kSize;
     const int64_t k = (int64_t)blockIdx.x * CPB + gid;

@@ -1,0 +1,40 @@
+// Run-time generated, mechanism-specialised kernels (jit.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "rtc_base.cuh"
+
+namespace hc {
+
+// host copy of the mechanism tables in the device order (reactions regrouped
+// by rate class, as uploaded to DevMech)
+struct HostMech {
+    int nsp = 0, nrc = 0;
+    std::vector<double> W, Trange, nasa;
+    std::vector<int32_t> rate_type, reversible, nf, nb, fidx, bidx;
+    std::vector<double> arr, arr0, troe, eff, fnu, bnu, ford, bord, sum_stoi;
+};
+
+struct JitKernel {
+    void *module = nullptr;   // CUmodule
+    void *func = nullptr;     // CUfunction
+    int N = 0, block = 0;
+    size_t smem = 0;
+    int per_sm = 0;
+};
+
+std::string jit_t1_source(const HostMech &h, int block);
+// NVRTC compile of generated source to an sm_100a cubin (host only)
+int jit_compile(const std::string &src, std::vector<char> &cubin, std::string &err);
+// compile (NVRTC, sm_100a) and load the thread-per-cell kernel for h;
+// modules are cached per source text for the life of the process
+int jit_build_t1(const HostMech &h, int block, JitKernel *out, std::string &err);
+int jit_launch_t1(const JitKernel &k, int num_sms, const IntegratorParams &P, const CellIO &io,
+                  double *ylast, cudaStream_t st, std::string &err);
+
+}  // namespace hc

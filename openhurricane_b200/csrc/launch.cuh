@@ -22,7 +22,7 @@ namespace hc {
 
 template <int N, int G>
 struct Launch {
-    static constexpr int kCellsPerBlock = (G == 64) ? 2 : 4;
+    static constexpr int kCellsPerBlock = cells_per_block(G);
     static size_t smem_bytes() { return sizeof(double) * Smem<N, G>::kSize * kCellsPerBlock; }
 
     static int integrate(const DevMech &m, int num_sms, const IntegratorParams &P,
@@ -36,7 +36,7 @@ struct Launch {
             err = "integrator kernel does not fit on an SM";
             return HC_E_UNSUPPORTED;
         }
-        const int64_t blocks_needed = (io.ncells + kCellsPerBlock - 1) / kCellsPerBlock;
+        const int64_t blocks_needed = (io.nqueue + kCellsPerBlock - 1) / kCellsPerBlock;
         const int64_t grid = std::min<int64_t>(blocks_needed, (int64_t)per_sm * num_sms);
         if (grid <= 0) return HC_OK;
         kern<<<(unsigned)grid, G * kCellsPerBlock, sm, st>>>(m, P, io);

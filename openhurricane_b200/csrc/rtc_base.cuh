@@ -1,0 +1,156 @@
+// Definitions shared by the precompiled kernels and the kernels generated
+// and compiled at run time for one mechanism (NVRTC): physical constants,
+// scalar helpers, rate-law formulas with their parameters passed by value,
+// and the integrator's parameter / field structures. Nothing here reads the
+// mechanism tables.
+#pragma once
+
+#ifndef __CUDACC_RTC__
+#include <cstdint>
+#include <cuda_runtime.h>
+#else
+typedef int int32_t;
+typedef long long int64_t;
+typedef unsigned long long uint64_t;
+#endif
+
+namespace hc {
+
+constexpr double kTiny = 1.0e-15;          // doubleRealTiny (doubleReal.hpp:43)
+constexpr double kVeryTiny = 1.0e-300;     // doubleRealVeryTiny
+constexpr double kVeryLarge = 1.0e+300;    // doubleRealVeryLarge
+constexpr double kRootVeryLarge = 1.0e+150;
+constexpr double kPatm = 1.01325e5;        // physicalConstant.hpp:186
+// Ru = (kB * NA) * 1e3 [J/kmol/K], evaluated like physicalConstant.hpp:158,183
+constexpr double kRu = (1.380649e-23 * 6.02214076e23) * 1e3;
+constexpr int kMaxSide = 4;
+
+enum RateType : int32_t { kArrhenius = 0, kThirdBody = 1, kLindemann = 2, kTroe3 = 3, kTroe4 = 4 };
+
+__device__ __forceinline__ double hmax(double a, double b) { return (a < b) ? b : a; }
+__device__ __forceinline__ double hmin(double a, double b) { return (b < a) ? b : a; }
+__device__ __forceinline__ double notZeroD(double s) { return (s != 0) ? s : kVeryTiny; }
+__device__ __forceinline__ bool finite(double x) { return !isnan(x) && !isinf(x); }
+
+// x^y, with the exponents mechanisms use in practice done exactly as a
+// correctly rounded pow returns them (y = 1: x; y = 2: one rounded multiply;
+// y = 0: 1; y = -1: one rounded division); any other exponent calls pow().
+__device__ __forceinline__ double pow_n(double x, double y) {
+    if (y == 1.0) return x;
+    if (y == 2.0) return x * x;
+    if (y == 0.0) return 1.0;
+    if (y == -1.0) return 1.0 / x;
+    return pow(x, y);
+}
+
+__device__ __forceinline__ double conc_pow(double c, double ord) {
+    return pow_n(hmax(c, 0.0), ord);
+}
+
+// ---------------------------------------------------------------- rate laws
+// ArrheniusRR::k (ArrheniusRR.cpp:37-47), A T^b e^{-Ta/T}, evaluated as one
+// exponential of b ln T - Ta/T with ln T shared by all reactions of a cell.
+__device__ __forceinline__ double arrK_log(double A, double b, double Ta, double T, double logT) {
+    double e = 0.0;
+    if (fabs(b) > kVeryTiny) e = b * logT;
+    if (fabs(Ta) > kVeryTiny) e -= Ta / T;
+    return A * exp(e);
+}
+
+__device__ __forceinline__ double troe_logfcent_p(double alpha, double Tsss, double Ts, double Tss,
+                                                  bool four, double T) {
+    double s = (1.0 - alpha) * exp(-T / Tsss) + alpha * exp(-T / Ts);
+    if (four) s += exp(-Tss / T);
+    return log10(hmax(s, kTiny));
+}
+
+// fallOffFunctions.cpp:81-100 (Troe::F); Lindemann F = 1
+__device__ __forceinline__ double fall_F(int type, double logFcent, double Pr) {
+    if (type == kLindemann) return 1.0;
+    const double c = -0.4 - 0.67 * logFcent;
+    const double n = 0.75 - 1.27 * logFcent;
+    const double d = 0.14;
+    const double logPr = log10(hmax(Pr, kTiny));
+    const double x = (logPr + c) / (n - d * (logPr + c));
+    return pow(10.0, logFcent / (1.0 + x * x));
+}
+
+// The Pr-independent product of Troe::DFDci (fallOffFunctions.cpp:102-129):
+// DFDci = [F * A * B * C] * (1/Pr * dPr/dci); returns F*A*B*C.
+__device__ __forceinline__ double troe_dfdci_factor(int type, double logFcent, double Pr,
+                                                    double F) {
+    if (type == kLindemann) return 0.0;
+    const double logPr = log10(hmax(Pr, kTiny));
+    const double c = -0.4 - 0.67 * logFcent;
+    const double n = 0.75 - 1.27 * logFcent;
+    const double d = 0.14;
+    const double logPrpc = logPr + c;
+    const double nm = n - d * logPrpc;
+    const double inv = logPrpc / nm;
+    const double s1 = 1.0 + inv * inv;
+    return F * ((-logFcent) / (s1 * s1)) * (2.0 * logPrpc / (nm * nm)) * (1.0 + d * inv);
+}
+
+// Troe::DFDT (fallOffFunctions.cpp:131-157)
+__device__ __forceinline__ double troe_dfdt_p(int type, double alpha, double Tsss, double Ts,
+                                              double Tss, double T, double Pr, double F,
+                                              double DPrDT) {
+    if (type == kLindemann) return 0.0;
+    const double ln10 = log(10.0);
+    const double logPr = log10(hmax(Pr, kTiny));
+    double Fcent, DFcentDT;
+    const double e1 = exp(-T / Tsss), e2 = exp(-T / Ts);
+    if (type == kTroe3) {
+        Fcent = hmax((1.0 - alpha) * e1 + alpha * e2, kTiny);
+        DFcentDT = (1.0 - alpha) * e1 / (-Tsss) + alpha * e2 / (-Ts);
+    } else {
+        const double e3 = exp(-Tss / T);
+        Fcent = hmax((1.0 - alpha) * e1 + alpha * e2 + e3, kTiny);
+        DFcentDT = (1.0 - alpha) * e1 / (-Tsss) + alpha * e2 / (-Ts) + e3 * (Tss / (T * T));
+    }
+    const double logFcent = log10(Fcent);
+    const double DlogFcentDT = 1.0 / (Fcent * ln10) * DFcentDT;
+    const double c = -0.4 - 0.67 * logFcent;
+    const double DcDT = -0.67 * DlogFcentDT;
+    const double n = 0.75 - 1.27 * logFcent;
+    const double DnDT = -1.27 * DlogFcentDT;
+    const double d = 0.14;
+    const double dlogPrDT = DPrDT / Pr / ln10;
+    const double logPrpc = logPr + c;
+    const double nm = n - d * logPrpc;
+    const double inv = logPrpc / nm;
+    const double dPPDT =
+        2.0 * logPrpc / (nm * nm) * ((dlogPrDT + DcDT) - logPrpc / nm * (DnDT - d * (dlogPrDT + DcDT)));
+    const double s1 = 1.0 + inv * inv;
+    return (F * ln10 * (DlogFcentDT / s1 - logFcent / (s1 * s1) * dPPDT));
+}
+
+struct IntegratorParams {
+    int32_t maxstep;
+    int32_t auto_update_jacobian;
+    int32_t step_to_update_jac;
+    double atol, rtol, safescale, minscale, maxscale, alphainc;
+    double atol_inc, rtol_inc, T_threshold, T_alpha, T_beta, dt_max;
+    double err_accept_limit;     // pow(maxscale/safescale, -1/alphainc)
+    int64_t max_newton_total;
+};
+
+struct CellIO {
+    int64_t ncells;         // field length (stride of species fields)
+    int64_t nqueue;         // cells to integrate: queue entries 0..nqueue-1
+    double *T;
+    const double *p;
+    double *rho;
+    double *Y;              // [nsp][ncells]
+    const double *dt;
+    double dt_factor;
+    double *subdt;
+    double *Ri;             // optional [nsp][ncells]
+    int32_t *status;        // optional
+    const int32_t *order;   // optional queue order (cell indices)
+    int64_t *cost;          // optional per-cell Newton iteration count out
+    unsigned long long *queue_head;
+    unsigned long long *counters;  // [6] n_jac, n_rhs, n_lu, n_newton, n_steps, n_attempts
+};
+
+}  // namespace hc

@@ -36,3 +36,10 @@ int launch_properties(const DevMech &m, int64_t n, const double *T, const double
                       const double *Y, double *ha, double *cp, double *mu, double *kappa,
                       double *D, cudaStream_t st, std::string &err);
 }
+
+namespace hc {
+struct T2Mech;
+}
+int variant_integrate_t2(int N, const hc::T2Mech &m, int num_sms, const hc::IntegratorParams &P,
+                         const hc::CellIO &io, double *ylast, int block, cudaStream_t st,
+                         std::string &err);

@@ -101,7 +101,8 @@ def _cells(tables, n, seed, **kw):
     return c.T, c.p, synth.mixture_density(tables.W, c), c.Y
 
 
-@pytest.mark.parametrize("kernel,block", [(0, 64), (1, 32), (1, 128), (2, 64)])
+@pytest.mark.parametrize("kernel,block", [(0, 64), (1, 32), (1, 128), (2, 64), (3, 32), (3, 128),
+                                          (4, 32), (4, 128)])
 def test_small_mechanism_parity_vs_oracle(small, kernel, block):
     t = small["tables"]
     T, p, rho, Y = _cells(t, 384, seed=11)
