@@ -136,10 +136,10 @@ const char *hc_last_error(void);
 void hc_default_opts(hc_opts *opts);
 
 /*
- * Kernel selection for hc_integrate*: kernel 0 = automatic (the compact
- * thread-per-cell kernel when nsp + 1 <= 16 and the mechanism fits its
- * tables, else the table-driven thread-per-cell kernel; a cell group of 32/64
- * lanes above 16 unknowns), 1 = table-driven thread per cell, 2 = cell group,
+ * Kernel selection for hc_integrate*: kernel 0 = automatic (the cell group:
+ * its lanes share each Newton iteration of one cell, which bounds the step's
+ * duration when per-cell costs are uneven), 1 = table-driven thread per
+ * cell, 2 = cell group (32 lanes up to 32 unknowns, 64 above),
  * 3 = thread per cell generated for this mechanism (every index and
  * coefficient a literal; compiled with NVRTC for sm_100a on first use, which
  * must precede any stream capture), 4 = compact thread per cell (mechanism

@@ -526,7 +526,13 @@ static int integrate_impl(hc_mech_t m, const hc_opts *opts, int64_t ncells, doub
         return fail(HC_E_UNSUPPORTED,
                     "compact thread-per-cell kernel needs nsp <= 15, <= 64 reactions and "
                     "autoUpdateJacobian off");
-    const bool use_t2 = t1_ok && m->t2_ok && (m->kernel == 4 || m->kernel == 0);
+    // automatic choice: the cell group. Per-cell costs in a flow step differ
+    // by orders of magnitude, and the step lasts as long as its stiffest
+    // cell; the cell group's lanes share each Newton iteration's work and
+    // finish a single cell several times sooner than one thread does, which
+    // outweighs the thread-per-cell kernels' higher throughput on uniform
+    // cells (measured on the batched workload).
+    const bool use_t2 = t1_ok && m->t2_ok && m->kernel == 4;
     if (use_t2) {
         if (m->ylast_cells < (size_t)ncells) {
             // grows only: a first call with a new, larger size synchronises the
@@ -557,7 +563,7 @@ static int integrate_impl(hc_mech_t m, const hc_opts *opts, int64_t ncells, doub
         if (m->kernel == 3) return fail(HC_E_UNSUPPORTED, "generated kernel unavailable: " + m->jit_err);
         use_jit = false;   // automatic choice: the precompiled thread-per-cell kernel
     }
-    const bool use_t1 = t1_ok && (m->kernel == 0 || m->kernel == 1 || use_jit);
+    const bool use_t1 = t1_ok && (m->kernel == 1 || use_jit);
     if (use_t1) {
         if (m->ylast_cells < (size_t)ncells) {
             // grows only: a first call with a new, larger size synchronises the

@@ -77,25 +77,92 @@ def make_large(n: int = 262144, seed: int = 3003, out_dir=None) -> Workload:
     return Workload("large", t, files, c.T, c.p, synth.mixture_density(t.W, c), c.Y, 1e-6)
 
 
+def gibbs_rt(t: MechTables, T: np.ndarray) -> np.ndarray:
+    """Molar standard Gibbs energy over Ru T of every species, [nsp, n], from
+    the NASA-7 polynomials (the mass-basis table divided by R_i)."""
+    T = np.asarray(T, np.float64)
+    out = np.empty((t.nsp, T.shape[0]))
+    for i in range(t.nsp):
+        hi = T >= t.Trange[i, 1]
+        a = np.where(hi[None, :], t.nasa[i, 1][:, None], t.nasa[i, 0][:, None]) / t.Ri[i]
+        h_rt = a[0] + a[1] * T / 2 + a[2] * T ** 2 / 3 + a[3] * T ** 3 / 4 + a[4] * T ** 4 / 5 + a[5] / T
+        s_r = a[0] * np.log(T) + a[1] * T + a[2] * T ** 2 / 2 + a[3] * T ** 3 / 3 + a[4] * T ** 4 / 4 + a[6]
+        out[i] = h_rt - s_r
+    return out
+
+
+def equilibrium_tp(t: MechTables, T, p, Y, iters: int = 200):
+    """Chemical equilibrium mass fractions at fixed T and p with the element
+    content of Y (element-potential method, damped Newton on the element
+    potentials and ln of the total moles, vectorised over cells). At the
+    equilibrium composition every reaction's forward and reverse rates
+    balance (Kc is built from the same Gibbs energies), so the state is a
+    fixed point of the reactor."""
+    T = np.asarray(T, np.float64)
+    p = np.asarray(p, np.float64)
+    A = t.elem_matrix[np.abs(t.elem_matrix).sum(axis=1) > 0]          # [ne, nsp]
+    ne = A.shape[0]
+    b = A @ (np.asarray(Y) / t.W[:, None])                             # kmol element / kg
+    g = gibbs_rt(t, T) + np.log(p / 101325.0)[None, :]                  # [nsp, n]
+    n = T.shape[0]
+    pi = np.zeros((ne, n))
+    nu = np.log(np.maximum(b.sum(axis=0), 1e-30))
+    present = (A.T @ (b > 0)) == A.sum(axis=0)[:, None]                  # species made of present elements
+    for _ in range(iters):
+        lx = -g + A.T @ pi
+        lx = np.where(present, np.minimum(lx, 50.0), -np.inf)
+        x = np.exp(lx)
+        nmol = np.exp(nu)[None, :] * x
+        Fe = A @ nmol - b
+        Fx = x.sum(axis=0) - 1.0
+        J = np.zeros((n, ne + 1, ne + 1))
+        J[:, :ne, :ne] = np.einsum("ei,fi,in->nef", A, A, nmol)
+        J[:, :ne, ne] = (A @ nmol).T
+        J[:, ne, :ne] = (A @ x).T
+        rhs = -np.concatenate([Fe, Fx[None, :]], axis=0).T              # [n, ne+1]
+        # elements absent from a cell: keep their potential fixed
+        absent = (b <= 0).T
+        for e in range(ne):
+            J[absent[:, e], e, :] = 0.0
+            J[absent[:, e], :, e] = 0.0
+            J[absent[:, e], e, e] = 1.0
+            rhs[absent[:, e], e] = 0.0
+        d = np.linalg.solve(J, rhs[..., None])[..., 0]
+        step = np.max(np.abs(d), axis=1)
+        lam = np.minimum(1.0, 2.0 / np.maximum(step, 1e-300))
+        pi += (lam[:, None] * d[:, :ne]).T
+        nu += lam * d[:, ne]
+        if np.max(step) < 1e-12:
+            break
+    lx = np.where(present, -g + A.T @ pi, -np.inf)
+    nmol = np.exp(nu)[None, :] * np.exp(lx)
+    Yeq = nmol * t.W[:, None]
+    return Yeq / Yeq.sum(axis=0, keepdims=True)
+
+
 def make_batched(n: int = 1048576, seed: int = 2002, frac_ignition: float = 0.2,
                  relax=None, pool: int = 8192, relax_time: float = 1e-4,
                  out_dir=None) -> Workload:
     """20 % ignition cells + 80 % near-equilibrium cells.
 
-    `relax(T, p, rho, Y, dt) -> (T, rho, Y)` integrates a pool of random
-    states over relax_time (the bench passes the GPU integrator); the pool is
-    then tiled over the near-equilibrium cells with a seeded jitter of
-    +-2 K in T so that no two cells are identical."""
+    Near-equilibrium cells come from a pool of random states: by default each
+    pool state is replaced by its chemical equilibrium at its own T and p
+    (equilibrium_tp; pool temperatures U[1500, 2800] K), or, when
+    `relax(T, p, rho, Y, dt) -> (T, rho, Y)` is given, by integrating it over
+    relax_time. The pool is tiled over the near-equilibrium cells with a
+    seeded jitter of +-2 K in T so that no two cells are identical."""
     _, files, t = mechanism_files("small", out_dir)
     rng = np.random.default_rng(seed)
     n_ign = int(round(frac_ignition * n))
     idx = [t.names.index(s) for s in REACTANTS_SMALL]
     ign = synth.ignition_cells(t.nsp, n_ign, seed=seed + 1, reactant_idx=idx)
     base = synth.dirichlet_cells(t.nsp, pool, seed=seed + 2)
-    rho_b = synth.mixture_density(t.W, base)
     if relax is None:
-        raise ValueError("make_batched needs a relax() integrator for the near-equilibrium pool")
-    Tb, rhob, Yb = relax(base.T, base.p, rho_b, base.Y, relax_time)
+        Tb = np.random.default_rng(seed + 3).uniform(1500.0, 2800.0, pool)
+        Yb = equilibrium_tp(t, Tb, base.p, base.Y)
+    else:
+        rho_b = synth.mixture_density(t.W, base)
+        Tb, rhob, Yb = relax(base.T, base.p, rho_b, base.Y, relax_time)
     n_eq = n - n_ign
     pick = rng.integers(0, pool, n_eq)
     T_eq = Tb[pick] + rng.uniform(-2.0, 2.0, n_eq)
