@@ -247,15 +247,18 @@ def integrate_device(mech, T, p, rho, Y, dt, opts=None):
 
 
 def generate_samples(mech, T, p, rho, Y, dt_nominal: float, n_samples: int, seed: int = 0,
-                     t_max: float = 3e-4, dt_spread: float = 3.0, opts=None):
+                     t_max: Optional[float] = None, dt_spread: float = 3.0, opts=None):
     """Training samples for the surrogate from the FP64 GPU integrator.
 
     Starting states (T, p, rho, Y: device arrays of base cells) are tiled to
-    n_samples, advanced along their own reaction trajectories by a random
-    time in [0, t_max] (so that states part-way through ignition appear), and
-    then integrated over a flow step dt drawn log-uniformly in
-    [dt_nominal / dt_spread, dt_nominal * dt_spread]. Returns the
-    pre-step state, dt and the increments (dT, dY)."""
+    n_samples; half of them are advanced along their own reaction
+    trajectories by a random time in [0, t_max] (default: one flow step, so
+    that states part-way through a step of ignition appear), and every
+    sample is then integrated over a flow step dt drawn log-uniformly in
+    [dt_nominal / dt_spread, dt_nominal * dt_spread]. Returns the pre-step
+    state, dt and the increments (dT, dY)."""
+    if t_max is None:
+        t_max = dt_nominal
     dev = T.device
     g = torch.Generator(device=dev).manual_seed(seed)
     nb = int(T.shape[0])
