@@ -209,6 +209,35 @@ int hc_integrate_subset(hc_mech_t mech, const hc_opts *opts, int64_t ncells, int
                         const double *dt, double dt_factor, double *subdt, double *Ri,
                         int32_t *status, int64_t *cost, hc_counters *counters, void *stream);
 
+/*
+ * Allocation-free integration. No counterpart in the reference.
+ *
+ * Same contract as hc_integrate (device pointers, stream-ordered) for
+ * mechanisms of nsp <= 15 species and <= 64 reactions, integrated with the
+ * compact thread-per-cell kernel, for callers that must not allocate device
+ * memory during the call: a solver that runs under a fixed device-memory
+ * budget or its own memory pool, code that calls the chemistry where the
+ * CUDA allocator must not be entered (a host callback, a section holding its
+ * own allocator's lock), or a loop that cannot afford the stream
+ * synchronisation a growing allocation brings. hc_integrate grows a per-cell
+ * scratch buffer with cudaMalloc when a call brings more cells than before;
+ * this call allocates nothing: its scratch is a fixed file-scope device array
+ * for at most HC_NOALLOC_MAX_CELLS cells (16 MiB, part of the library's
+ * device image, placed in device memory when the CUDA runtime loads that
+ * image), and larger calls are rejected with HC_E_INVALID. The first call on each device looks up that
+ * array's address (cudaGetSymbolAddress, with that device current); make it
+ * before any stream capture. The work queue in the array is zeroed with
+ * cudaMemsetAsync at every call. All calls share the array: calls that
+ * overlap in time (other streams, other host threads) race on it, so callers
+ * serialise them. Returns HC_OK or a negative HC_E_* code; per-cell statuses
+ * go to status (no count is returned, which would need a host copy).
+ */
+#define HC_NOALLOC_MAX_CELLS 65536
+int hc_integrate_noalloc(hc_mech_t mech, const hc_opts *opts, int64_t ncells, double *T,
+                         const double *p, double *rho, double *Y, const double *dt,
+                         double dt_factor, double *subdt, double *Ri, int32_t *status,
+                         void *stream);
+
 /* Same as hc_integrate with host buffers: H2D, integrate, D2H, synchronise. */
 int hc_integrate_host(hc_mech_t mech, const hc_opts *opts, int64_t ncells, double *T,
                       const double *p, double *rho, double *Y, const double *dt, double dt_factor,

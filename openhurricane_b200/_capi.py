@@ -80,6 +80,8 @@ SIGNATURES = {
                              [C.c_double] + [_VP] * 6 + [_VP]),
     "hc_integrate_subset": (C.c_int, [_VP, C.POINTER(HcOpts), C.c_int64, C.c_int64, _VP] +
                             [_VP] * 5 + [C.c_double] + [_VP] * 5 + [_VP]),
+    "hc_integrate_noalloc": (C.c_int, [_VP, C.POINTER(HcOpts), C.c_int64] + [_VP] * 5 +
+                             [C.c_double] + [_VP] * 3 + [_VP]),
     "hc_integrate_host": (C.c_int, [_VP, C.POINTER(HcOpts), C.c_int64] + [_VP] * 5 +
                           [C.c_double] + [_VP] * 4 + [_VP]),
     "hc_rhs_jacobian": (C.c_int, [_VP, C.c_int64] + [_VP] * 5 + [_VP]),
@@ -103,6 +105,9 @@ SIGNATURES = {
 }
 
 _lib: Optional[C.CDLL] = None
+
+
+NOALLOC_MAX_CELLS = 65536   # HC_NOALLOC_MAX_CELLS
 
 
 class HcError(RuntimeError):

@@ -833,3 +833,92 @@ int hc_surrogate_gate(hc_mech_t m, int64_t n, double *T, const double *p, double
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free integration (hc_integrate_noalloc).
+//
+// For callers that must not allocate device memory during the call: a flow
+// solver running under a fixed device-memory budget or a memory pool it
+// manages itself, code that calls the chemistry from inside a region where
+// the CUDA allocator must not be entered (a host callback, a section holding
+// its own allocator's lock), or a real-time loop that cannot afford the
+// synchronisation a growing allocation brings. hc_integrate keeps a per-cell
+// scratch buffer in the mechanism handle and grows it with cudaMalloc (after
+// a stream synchronisation) whenever a call brings more cells than before;
+// this entry point never does: its scratch is the file-scope device array
+// below, of a fixed size stated by HC_NOALLOC_MAX_CELLS.
+//
+// Scratch layout: the two previous step states of every cell (ImplicitEuler's
+// yklast_, 2 x 16 doubles per cell) for HC_NOALLOC_MAX_CELLS cells, then the
+// work-queue head and the six work counters (8 words reserved), which are
+// zeroed with cudaMemsetAsync at every call (the per-cell states need no
+// initialisation: each is written before it is read). Every call uses the
+// same array, so calls that overlap in time (concurrent streams, or several
+// host threads) race on it; callers serialise their calls.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoAllocYlast = 2 * 16 * (size_t)HC_NOALLOC_MAX_CELLS;   // doubles
+__device__ __align__(256) double g_noalloc_scratch[kNoAllocYlast + 8];
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[256] = {};   // the array's device address, per device
+
+}  // namespace
+
+extern "C" int hc_integrate_noalloc(hc_mech_t m, const hc_opts *opts, int64_t ncells, double *T,
+                                    const double *p, double *rho, double *Y, const double *dt,
+                                    double dt_factor, double *subdt, double *Ri, int32_t *status,
+                                    void *stream) {
+    if (!m) return fail(HC_E_INVALID, "null mechanism");
+    int rc = check_opts(opts);
+    if (rc != HC_OK) return rc;
+    if (ncells < 0) return fail(HC_E_INVALID, "negative cell count");
+    if (ncells > HC_NOALLOC_MAX_CELLS)
+        return fail(HC_E_INVALID, "hc_integrate_noalloc takes at most HC_NOALLOC_MAX_CELLS (" +
+                                      std::to_string(HC_NOALLOC_MAX_CELLS) + ") cells per call, got " +
+                                      std::to_string(ncells));
+    if (ncells == 0) return HC_OK;
+    if (!T || !p || !rho || !Y || !dt || !subdt) return fail(HC_E_INVALID, "null field");
+    if (!(dt_factor > 0)) return fail(HC_E_INVALID, "dt_factor must be positive");
+    const int N = m->dm.nsp + 1;
+    if (N > 16 || opts->auto_update_jacobian || !m->t2_ok)
+        return fail(HC_E_UNSUPPORTED,
+                    "hc_integrate_noalloc needs nsp <= 15, <= 64 reactions and autoUpdateJacobian off");
+    int dev = -1;
+    HC_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) return fail(HC_E_CUDA, "device ordinal out of range");
+    void *base = nullptr;
+    {
+        // the array's address is looked up once per device, with that device current
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            void *a = nullptr;
+            HC_CUDA(cudaGetSymbolAddress(&a, g_noalloc_scratch));
+            g_noalloc_addr[dev] = a;
+        }
+        base = g_noalloc_addr[dev];
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    double *ylast = static_cast<double *>(base);
+    unsigned long long *queue = reinterpret_cast<unsigned long long *>(ylast + kNoAllocYlast);
+    HC_CUDA(cudaMemsetAsync(queue, 0, 8 * sizeof(unsigned long long), st));
+    CellIO io;
+    io.ncells = ncells;
+    io.nqueue = ncells;
+    io.T = T;
+    io.p = p;
+    io.rho = rho;
+    io.Y = Y;
+    io.dt = dt;
+    io.dt_factor = dt_factor;
+    io.subdt = subdt;
+    io.Ri = Ri;
+    io.status = status;
+    io.order = nullptr;
+    io.cost = nullptr;
+    io.queue_head = queue;
+    io.counters = queue + 1;
+    const IntegratorParams P = make_params(opts);
+    return variant_integrate_t2(N, m->t2, m->num_sms, P, io, ylast, m->block, st, g_err);
+}
