@@ -364,7 +364,7 @@ def surrogate_leg(args, wl, mech, fields0, dt, fp64_ref, plain_ms, flush, rank):
                            args.sur_samples, seed=11 + rank, opts=opts)
     torch.cuda.synchronize()
     t_gen = time.perf_counter() - t0
-    sur = Surrogate(mech, n_hidden=3, width=256, max_batch=65536, seed=3 + rank)
+    sur = Surrogate(mech, n_hidden=3, width=256, max_batch=65536, seed=3 + rank, n_ensemble=3)
     sur.fit_normalisation(smp["T"], smp["p"], smp["Y"], smp["dt"], smp["dT"], smp["dY"])
     X = sur.features(smp["T"], smp["p"], smp["Y"], smp["dt"])
     D = sur.targets(smp["dT"], smp["dY"])
@@ -413,7 +413,9 @@ def surrogate_leg(args, wl, mech, fields0, dt, fp64_ref, plain_ms, flush, rank):
             bool(acc.any()) else 0.0,
             "linf_dY": float(dY.max()),
             "max_element_rel_err_accepted": float(rel[:, acc].max()) if bool(acc.any()) else 0.0,
-            "network": "13 -> 3 x 256 GELU -> 10, BF16 tcgen05 / FP32 accumulate",
+            "network": "12 -> 3 x 256 GELU -> 10 (x3 ensemble), BF16 tcgen05 / FP32 accumulate",
+            "gate": {"tol_T_K": sur.gate.tol_T, "spread_T_K": sur.spread_T,
+                     "spread_Y": sur.spread_Y, "y_neg": sur.gate.y_neg},
             "train_samples": n_train, "train_epochs": args.sur_epochs, "batch": 8192,
             "final_loss": losses[-1] if losses else None,
             "sample_gen_s": t_gen, "train_s": t_train,
@@ -477,8 +479,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--surrogate", type=int, default=1,
                     help="1: also train and time the gated surrogate (batched workload)")
-    ap.add_argument("--sur-samples", type=int, default=4194304)
-    ap.add_argument("--sur-epochs", type=int, default=4)
+    ap.add_argument("--sur-samples", type=int, default=524288)
+    ap.add_argument("--sur-epochs", type=int, default=150)
     args = ap.parse_args()
     if args.warmup < 1:
         raise SystemExit("--warmup must be >= 1")

@@ -324,17 +324,21 @@ int hc_gemm_bf16_tn(const void *A, const void *B, int M, int N, int K, const flo
 /*
  * Surrogate path around the network (no reference counterpart).
  *
- * hc_surrogate_features: X[n][nsp+3] (float) = normalised (T, ln p, Y_1..Y_nsp,
- * ln(dt*dt_factor)): (value - mean[j]) * inv_std[j].
+ * hc_surrogate_features: X[n][nsp+3] (float) = normalised (T, ln p,
+ * ln max(Y_1, 1e-20) .. ln max(Y_nsp, 1e-20), ln(dt*dt_factor)):
+ * (value - mean[j]) * inv_std[j].
  *
  * hc_surrogate_gate: pred[n][nsp+1] is the network's normalised increment
  * (dT, dY_1..dY_nsp) over the flow step (de-normalised with out_mean /
  * out_std). Per cell, in FP64: dY is projected onto the element-conserving
  * subspace with proj[nsp][nsp]; Y' = Y + dY (components below -y_neg reject,
- * those in [-y_neg, 0) become 0); T' solves sum Y'_i h_i(T') = sum Y_i h_i(T)
+ * those in [-y_neg, 0) become 0 and the element mass they carried is taken
+ * from the major species, Y' > 1e-3, with elem[nel][nsp] = atoms / W);
+ * T' solves sum Y'_i h_i(T') = sum Y_i h_i(T)
  * (constant-pressure enthalpy); the cell is accepted when |T' - (T + dT)| <=
  * tol_T, the projection moved dY by at most tol_proj * max(|dY|_inf, 1e-6),
- * every |X| <= x_max and T_min < T' < T_max. Accepted cells get T', Y' and
+ * every |X| <= x_max, T_min < T' < T_max and, when spread != NULL (an
+ * ensemble's per-cell disagreement), spread <= tol_spread. Accepted cells get T', Y' and
  * rho = p/(R_m T'); rejected cells are untouched, listed in rejected[0..
  * *n_rejected) (any order) for hc_integrate_subset. Synchronises the stream.
  */
@@ -344,6 +348,7 @@ typedef struct hc_gate_opts {
     double y_neg;     /* largest negative mass fraction clipped to zero */
     double x_max;     /* input features' range, in training standard deviations */
     double T_min, T_max;
+    double tol_spread; /* largest ensemble disagreement accepted */
 } hc_gate_opts;
 
 int hc_surrogate_features(hc_mech_t mech, int64_t n, const double *T, const double *p,
@@ -351,8 +356,9 @@ int hc_surrogate_features(hc_mech_t mech, int64_t n, const double *T, const doub
                           const double *inv_std, float *X, void *stream);
 int hc_surrogate_gate(hc_mech_t mech, int64_t n, double *T, const double *p, double *rho,
                       double *Y, const float *pred, const float *X, const double *out_mean,
-                      const double *out_std, const double *proj, const hc_gate_opts *gate,
-                      int32_t *accept, int32_t *rejected, int64_t *n_rejected, void *stream);
+                      const double *out_std, const double *proj, const double *elem, int nel,
+                      const float *spread, const hc_gate_opts *gate, int32_t *accept,
+                      int32_t *rejected, int64_t *n_rejected, void *stream);
 
 #ifdef __cplusplus
 }

@@ -49,7 +49,7 @@ class HcOpts(C.Structure):
 
 class HcGateOpts(C.Structure):
     _fields_ = [(k, C.c_double) for k in ("tol_T", "tol_proj", "y_neg", "x_max", "T_min",
-                                          "T_max")]
+                                          "T_max", "tol_spread")]
 
 
 class HcCounters(C.Structure):
@@ -100,7 +100,7 @@ SIGNATURES = {
     "hc_mlp_forward": (C.c_int, [_VP, _VP, C.c_int64, _VP, _VP]),
     "hc_mlp_check": (C.c_int, [_VP, _VP]),
     "hc_surrogate_features": (C.c_int, [_VP, C.c_int64] + [_VP] * 4 + [C.c_double] + [_VP] * 4),
-    "hc_surrogate_gate": (C.c_int, [_VP, C.c_int64] + [_VP] * 14),
+    "hc_surrogate_gate": (C.c_int, [_VP, C.c_int64] + [_VP] * 10 + [C.c_int] + [_VP] * 6),
     "hc_gemm_bf16_tn": (C.c_int, [_VP, _VP, C.c_int, C.c_int, C.c_int, _VP, C.c_int, _VP, _VP]),
 }
 

@@ -791,15 +791,17 @@ int hc_surrogate_features(hc_mech_t m, int64_t n, const double *T, const double 
 
 int hc_surrogate_gate(hc_mech_t m, int64_t n, double *T, const double *p, double *rho, double *Y,
                       const float *pred, const float *X, const double *out_mean,
-                      const double *out_std, const double *proj, const hc_gate_opts *g,
-                      int32_t *accept, int32_t *rejected, int64_t *n_rejected, void *stream) {
+                      const double *out_std, const double *proj, const double *elem, int nel,
+                      const float *spread, const hc_gate_opts *g, int32_t *accept,
+                      int32_t *rejected, int64_t *n_rejected, void *stream) {
     if (!m) return fail(HC_E_INVALID, "null mechanism");
     if (!g || !n_rejected) return fail(HC_E_INVALID, "null argument");
     *n_rejected = 0;
     if (n <= 0) return HC_OK;
-    if (!T || !p || !rho || !Y || !pred || !X || !out_mean || !out_std || !proj || !accept ||
-        !rejected)
+    if (!T || !p || !rho || !Y || !pred || !X || !out_mean || !out_std || !proj || !elem ||
+        !accept || !rejected)
         return fail(HC_E_INVALID, "null field");
+    if (nel < 1 || nel > 8) return fail(HC_E_INVALID, "the gate handles 1 to 8 elements");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     unsigned long long *cnt = m->queue + 7;
     HC_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), st));
@@ -814,12 +816,16 @@ int hc_surrogate_gate(hc_mech_t m, int64_t n, double *T, const double *p, double
     a.out_mean = out_mean;
     a.out_std = out_std;
     a.proj = proj;
+    a.elem = elem;
+    a.nel = nel;
     a.tol_T = g->tol_T;
     a.tol_proj = g->tol_proj;
     a.y_neg = g->y_neg;
     a.x_max = g->x_max;
     a.T_min = g->T_min;
     a.T_max = g->T_max;
+    a.spread = spread;
+    a.tol_spread = g->tol_spread;
     a.accept = accept;
     a.rejected = rejected;
     a.n_rejected = cnt;

@@ -9,7 +9,9 @@
 //      / W_i (P is built on the host); this also makes sum_i dY_i = 0, since
 //      W_i = sum_e (atoms) * (atomic weight);
 //   3. Y' = Y + dY; a component below -y_neg rejects the cell, components in
-//      [-y_neg, 0) are set to 0;
+//      [-y_neg, 0) are set to 0, and the element mass those clipped
+//      components carried is taken from the major species (Y' > 1e-3) by the
+//      minimum-norm correction on them, so elements stay conserved;
 //   4. T' from the conserved mixture enthalpy of the constant-pressure
 //      reactor, sum_i Y'_i h_i(T') = sum_i Y_i h_i(T), by Newton's method on
 //      the NASA-7 polynomials (thermoList::THa_p, thermoList.cpp:470-533),
@@ -17,8 +19,9 @@
 //   5. accept when |T' - (T + dT_p)| <= tol_T (the network's temperature
 //      agrees with the conserved enthalpy), the projection changed the
 //      prediction by at most tol_proj * max(|dY_p|_inf, 1e-6), every input
-//      feature lies within +-x_max standard deviations of the training data
-//      and T' lies in [T_min, T_max];
+//      feature lies within +-x_max standard deviations of the training data,
+//      T' lies in [T_min, T_max] and, when an ensemble's disagreement is
+//      given, it is at most tol_spread;
 //   6. accepted cells get T', Y' and rho = p / (R_m T'); rejected cells are
 //      left untouched and appended to the rejected-cell list.
 #include <cuda_runtime.h>
@@ -37,6 +40,8 @@ void set_last_error(const std::string &msg);
 namespace hc {
 
 constexpr int kSurMaxSp = 64;
+constexpr int kSurMaxEl = 8;
+constexpr double kSurYFloor = 1e-20;   // mass fractions enter the network as ln(max(Y, floor))
 
 __global__ void features_kernel(int nsp, int64_t n, const double *__restrict__ T,
                                 const double *__restrict__ p, const double *__restrict__ Y,
@@ -49,8 +54,10 @@ __global__ void features_kernel(int nsp, int64_t n, const double *__restrict__ T
         float *x = X + c * n_in;
         x[0] = (float)((T[c] - mean[0]) * inv_std[0]);
         x[1] = (float)((log(p[c]) - mean[1]) * inv_std[1]);
-        for (int i = 0; i < nsp; ++i)
-            x[2 + i] = (float)((Y[(int64_t)i * n + c] - mean[2 + i]) * inv_std[2 + i]);
+        for (int i = 0; i < nsp; ++i) {
+            const double yi = Y[(int64_t)i * n + c];
+            x[2 + i] = (float)((log(yi > kSurYFloor ? yi : kSurYFloor) - mean[2 + i]) * inv_std[2 + i]);
+        }
         x[n_in - 1] = (float)((log(dt[c] * dt_factor) - mean[n_in - 1]) * inv_std[n_in - 1]);
     }
 }
@@ -62,6 +69,7 @@ __global__ void gate_kernel(const __grid_constant__ DevMech m, const __grid_cons
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < a.n;
          c += (int64_t)gridDim.x * blockDim.x) {
         bool ok = true;
+        if (a.spread && !(a.spread[c] <= (float)a.tol_spread)) ok = false;
         for (int j = 0; j < n_in; ++j) {
             const float x = a.X[c * n_in + j];
             if (!(fabsf(x) <= (float)a.x_max)) ok = false;
@@ -92,6 +100,67 @@ __global__ void gate_kernel(const __grid_constant__ DevMech m, const __grid_cons
             y[i] = (yi < 0.0) ? 0.0 : yi;
         }
         if (corr > a.tol_proj * hmax(pmax, 1e-6)) ok = false;
+        // element mass of the clipped components, returned through the major species
+        if (ok) {
+            const int ne = a.nel;
+            double r[kSurMaxEl];
+            bool clipped = false;
+            for (int e = 0; e < ne; ++e) r[e] = 0.0;
+            for (int i = 0; i < nsp; ++i) {
+                double d = 0.0;
+                for (int k = 0; k < nsp; ++k) d += a.proj[i * nsp + k] * dyp[k];
+                const double ex = a.Y[(int64_t)i * a.n + c] + d;   // unclipped
+                if (y[i] != ex) {
+                    clipped = true;
+                    for (int e = 0; e < ne; ++e) r[e] += a.elem[e * nsp + i] * (y[i] - ex);
+                }
+            }
+            if (clipped) {
+                // (A_S A_S^T) lam = r over the major species S, then y_S -= A_S^T lam
+                double M[kSurMaxEl][kSurMaxEl + 1];
+                for (int e = 0; e < ne; ++e) {
+                    for (int f = 0; f < ne; ++f) {
+                        double sum = 0.0;
+                        for (int i = 0; i < nsp; ++i)
+                            if (y[i] > 1e-3) sum += a.elem[e * nsp + i] * a.elem[f * nsp + i];
+                        M[e][f] = sum;
+                    }
+                    M[e][ne] = r[e];
+                }
+                bool solvable = true;
+                for (int k = 0; k < ne && solvable; ++k) {
+                    int pv = k;
+                    for (int i = k + 1; i < ne; ++i)
+                        if (fabs(M[i][k]) > fabs(M[pv][k])) pv = i;
+                    if (!(fabs(M[pv][k]) > 1e-300)) {
+                        // an element without a major carrier: its residual must already be 0
+                        if (fabs(M[pv][ne]) > 0.0) solvable = false;
+                        for (int j = 0; j <= ne; ++j) M[pv][j] = (j == k) ? 1.0 : 0.0;
+                    }
+                    if (pv != k)
+                        for (int j = 0; j <= ne; ++j) {
+                            const double tmp = M[k][j];
+                            M[k][j] = M[pv][j];
+                            M[pv][j] = tmp;
+                        }
+                    for (int i = 0; i < ne; ++i) {
+                        if (i == k) continue;
+                        const double l = M[i][k] / M[k][k];
+                        for (int j = k; j <= ne; ++j) M[i][j] -= l * M[k][j];
+                    }
+                }
+                if (!solvable) {
+                    ok = false;
+                } else {
+                    for (int i = 0; i < nsp; ++i) {
+                        if (!(y[i] > 1e-3)) continue;
+                        double adj = 0.0;
+                        for (int e = 0; e < ne; ++e) adj += a.elem[e * nsp + i] * (M[e][ne] / M[e][e]);
+                        y[i] -= adj;
+                    }
+                }
+            }
+        }
         // T' from sum Y' h(T') = h0
         double Tn = T0 + dTp;
         if (!(Tn > a.T_min && Tn < a.T_max)) ok = false;

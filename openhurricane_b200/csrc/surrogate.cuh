@@ -21,7 +21,11 @@ struct GateArgs {
     const double *out_mean;    // [nsp+1]
     const double *out_std;     // [nsp+1]
     const double *proj;        // [nsp][nsp]
+    const double *elem;        // [nel][nsp] atoms of element e per kg of species i (E / W)
+    int nel;
     double tol_T, tol_proj, y_neg, x_max, T_min, T_max;
+    const float *spread;       // [n] ensemble disagreement (optional), accept <= tol_spread
+    double tol_spread;
     int32_t *accept;           // [n] 1 accepted, 0 rejected
     int32_t *rejected;         // [n] list of rejected cells
     unsigned long long *n_rejected;

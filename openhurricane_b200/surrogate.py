@@ -1,8 +1,8 @@
 """Learned chemistry surrogate: the network (hc_mlp_* of the C ABI) and the
 host side of its training and gated inference.
 
-The network maps a cell state and the flow step (T, log p, Y_1..Y_nsp,
-log dt), normalised, to the normalised chemistry increment (dT, dY_1..dY_nsp)
+The network maps a cell state and the flow step (T, ln p, ln Y_1..ln Y_nsp,
+ln dt), normalised, to the normalised chemistry increment (dT, dY_1..dY_nsp)
 over that step. Its forward and backward passes are the library's BF16
 tcgen05 kernels accumulating in FP32; parameters are FP32 with Adam.
 """
@@ -136,21 +136,33 @@ class Surrogate:
     cells are integrated by the FP64 integrator (hc_integrate_subset)."""
 
     def __init__(self, mech, n_hidden: int = 3, width: int = 256, max_batch: int = 65536,
-                 seed: int = 0):
+                 seed: int = 0, n_ensemble: int = 3):
         self.mech = mech
         t = mech.tables
         self.nsp = t.nsp
         self.n_in, self.n_out = t.nsp + 3, t.nsp + 1
-        self.net = MLP(self.n_in, self.n_out, n_hidden, width, max_batch=max_batch, seed=seed)
+        # an ensemble of networks trained from different initialisations and
+        # batch orders: their disagreement is the gate's confidence measure
+        self.nets = [MLP(self.n_in, self.n_out, n_hidden, width, max_batch=max_batch,
+                         seed=seed + 1000 * k) for k in range(n_ensemble)]
+        self.net = self.nets[0]
+        # disagreement scales: a cell is rejected when the ensemble's spread
+        # in dT exceeds spread_T (K) or in any dY exceeds spread_Y
+        self.spread_T = 1.0
+        self.spread_Y = 1e-2
         dev = torch.device("cuda", torch.cuda.current_device())
         self.dev = dev
         self.proj = torch.tensor(element_projector(t), dtype=torch.float64, device=dev)
+        A = t.elem_matrix / t.W[None, :]
+        A = A[np.abs(A).sum(axis=1) > 0]
+        self.elem = torch.tensor(np.ascontiguousarray(A), dtype=torch.float64, device=dev)
+        self.nel = int(A.shape[0])
         self.in_mean = torch.zeros(self.n_in, dtype=torch.float64, device=dev)
         self.in_istd = torch.ones(self.n_in, dtype=torch.float64, device=dev)
         self.out_mean = torch.zeros(self.n_out, dtype=torch.float64, device=dev)
         self.out_std = torch.ones(self.n_out, dtype=torch.float64, device=dev)
-        self.gate = _capi.HcGateOpts(tol_T=2.0, tol_proj=0.5, y_neg=1e-12, x_max=8.0, T_min=250.0,
-                                     T_max=4000.0)
+        self.gate = _capi.HcGateOpts(tol_T=2.0, tol_proj=0.5, y_neg=1e-4, x_max=8.0, T_min=250.0,
+                                     T_max=4000.0, tol_spread=1.0)
 
     # ------------------------------------------------------------------ data
     def features(self, T, p, Y, dt, dt_factor: float = 1.0, out=None) -> torch.Tensor:
@@ -165,7 +177,9 @@ class Surrogate:
 
     @staticmethod
     def raw_features(T, p, Y, dt):
-        return torch.cat([T[None], torch.log(p)[None], Y, torch.log(dt)[None]], dim=0).T
+        """(T, ln p, ln max(Y_i, 1e-20), ln dt) per cell, as hc_surrogate_features."""
+        lY = torch.log(torch.clamp(Y, min=1e-20))
+        return torch.cat([T[None], torch.log(p)[None], lY, torch.log(dt)[None]], dim=0).T
 
     def fit_normalisation(self, T, p, Y, dt, dT, dY):
         """Input / output statistics of the training set (float64)."""
@@ -183,29 +197,44 @@ class Surrogate:
         return ((d - self.out_mean) / self.out_std).to(torch.float32).contiguous()
 
     # ------------------------------------------------------------------ train
-    def train(self, X: torch.Tensor, D: torch.Tensor, epochs: int = 4, batch: int = 8192,
-              lr: float = 2e-3, lr_final: float = 5e-5, seed: int = 0, log=None):
-        """Adam over shuffled mini-batches with a cosine learning-rate decay."""
+    def train(self, X: torch.Tensor, D: torch.Tensor, epochs: int = 150, batch: int = 8192,
+              lr: float = 2e-3, lr_final: float = 2e-5, seed: int = 0, log=None):
+        """Adam over shuffled mini-batches with a cosine learning-rate decay,
+        every network of the ensemble with its own batch order. Returns the
+        first network's loss at the end of each epoch."""
         n = int(X.shape[0])
         steps_per_epoch = max(1, n // batch)
         total = epochs * steps_per_epoch
-        g = torch.Generator(device=X.device).manual_seed(seed)
-        k = 0
         losses = []
-        for ep in range(epochs):
-            perm = torch.randperm(n, device=X.device, generator=g)
-            for s in range(steps_per_epoch):
-                idx = perm[s * batch:(s + 1) * batch]
-                xb, yb = X[idx].contiguous(), D[idx].contiguous()
-                a = lr_final + 0.5 * (lr - lr_final) * (1 + np.cos(np.pi * k / max(1, total)))
-                want = (s == steps_per_epoch - 1)
-                l = self.net.train_step(xb, yb, a, want_loss=want, check=want)
-                if want:
-                    losses.append(l)
-                    if log:
-                        log(f"epoch {ep} loss {l:.4e}")
-                k += 1
+        for m, net in enumerate(self.nets):
+            g = torch.Generator(device=X.device).manual_seed(seed + 7919 * m)
+            k = 0
+            for ep in range(epochs):
+                perm = torch.randperm(n, device=X.device, generator=g)
+                for s in range(steps_per_epoch):
+                    idx = perm[s * batch:(s + 1) * batch]
+                    xb, yb = X[idx].contiguous(), D[idx].contiguous()
+                    a = lr_final + 0.5 * (lr - lr_final) * (1 + np.cos(np.pi * k / max(1, total)))
+                    want = (s == steps_per_epoch - 1) and (m == 0 or ep == epochs - 1)
+                    l = net.train_step(xb, yb, a, want_loss=want, check=want)
+                    if want and m == 0:
+                        losses.append(l)
+                        if log:
+                            log(f"epoch {ep} loss {l:.4e}")
+                    k += 1
         return losses
+
+    def predict(self, X: torch.Tensor):
+        """Mean normalised prediction of the ensemble and its per-cell
+        disagreement (the larger of the dT spread / spread_T and the largest
+        dY spread / spread_Y; <= 1 is confident)."""
+        preds = torch.stack([net.forward(X) for net in self.nets])
+        mean = preds.mean(dim=0).contiguous()
+        if len(self.nets) == 1:
+            return mean, None
+        rng = (preds.max(dim=0).values - preds.min(dim=0).values).double() * self.out_std[None, :]
+        sp = torch.maximum(rng[:, 0] / self.spread_T, rng[:, 1:].max(dim=1).values / self.spread_Y)
+        return mean, sp.to(torch.float32).contiguous()
 
     # ------------------------------------------------------------------ infer
     def step(self, flow, dt: torch.Tensor, dt_factor: float = 1.0, opts=None,
@@ -214,14 +243,21 @@ class Surrogate:
         place). Returns (n_rejected, accept mask)."""
         n = flow.n
         X = self.features(flow.T, flow.p, flow.Y, dt, dt_factor)
-        pred = self.net.forward(X)
+        pred, spread = self.predict(X)
+        return self.apply(flow, dt, X, pred, spread, dt_factor, opts, subdt)
+
+    def apply(self, flow, dt, X, pred, spread, dt_factor: float = 1.0, opts=None, subdt=None):
+        """The gate and the FP64 fallback for a given prediction."""
+        n = flow.n
         accept = torch.empty(n, dtype=torch.int32, device=flow.T.device)
         rejected = torch.empty(n, dtype=torch.int32, device=flow.T.device)
         nrej = C.c_int64(0)
         _capi.check(_capi.load().hc_surrogate_gate(
             self.mech.handle, n, _vp(flow.T), _vp(flow.p), _vp(flow.rho), _vp(flow.Y), _vp(pred),
-            _vp(X), _vp(self.out_mean), _vp(self.out_std), _vp(self.proj), C.byref(self.gate),
-            _vp(accept), _vp(rejected), C.byref(nrej), _vp_stream()), "hc_surrogate_gate")
+            _vp(X), _vp(self.out_mean), _vp(self.out_std), _vp(self.proj), _vp(self.elem),
+            self.nel, _vp(spread), C.byref(self.gate), _vp(accept), _vp(rejected), C.byref(nrej),
+            _vp_stream()),
+            "hc_surrogate_gate")
         nr = int(nrej.value)
         if nr > 0:
             o = opts if opts is not None else _capi.default_opts()

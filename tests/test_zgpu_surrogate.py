@@ -41,12 +41,12 @@ def test_gated_surrogate_small_mechanism(small):
     d = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
     s = generate_samples(mech, d(base.T), d(base.p), d(base.rho), d(base.Y), 1e-5, 131072,
                          seed=1, opts=opts)
-    sur = Surrogate(mech, n_hidden=3, width=256, max_batch=65536, seed=2)
+    sur = Surrogate(mech, n_hidden=3, width=256, max_batch=65536, seed=2, n_ensemble=3)
     sur.fit_normalisation(s["T"], s["p"], s["Y"], s["dt"], s["dT"], s["dY"])
     X = sur.features(s["T"], s["p"], s["Y"], s["dt"])
     D = sur.targets(s["dT"], s["dY"])
-    losses = sur.train(X, D, epochs=6, batch=8192, lr=2e-3)
-    assert losses[-1] < 0.5 * losses[0]
+    losses = sur.train(X, D, epochs=120, batch=8192, lr=2e-3)
+    assert losses[-1] < 0.6 * losses[0]
 
     test = workloads.make_batched(32768, seed=99, pool=2048)
     n = test.n
@@ -60,6 +60,7 @@ def test_gated_surrogate_small_mechanism(small):
     acc = accept.bool()
     dT = (flow.T - ref.T).abs()
     print(f"rejected {nrej}/{n}, max|dT| accepted {dT[acc].max().item():.3f} K")
+    assert nrej < n                     # the network takes part
     assert dT.max().item() < 5.0
     # rejected cells: the FP64 integrator's own result
     assert torch.equal(flow.T[~acc], ref.T[~acc])
