@@ -13,7 +13,8 @@ from typing import Optional
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libhurchem_b200.so")
+# HURCHEM_B200_LIB selects another build of the library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("HURCHEM_B200_LIB") or os.path.join(HERE, "libhurchem_b200.so")
 
 HC_MAX_SIDE = 4
 HC_CELL_OK = 0

@@ -656,7 +656,10 @@ __device__ __forceinline__ Group<G> make_group(double *s, int gid, int red_off, 
 __device__ const IntegratorParams kNoParams{};
 
 template <int N, int G>
-__global__ void __launch_bounds__(128, (G == 64) ? 2 : 3)
+#ifndef HC_GROUP_MIN_BLOCKS
+#define HC_GROUP_MIN_BLOCKS 4   // blocks of 128 threads per SM the 32-lane groups are built for (measured best)
+#endif
+__global__ void __launch_bounds__(128, (G == 64) ? 2 : HC_GROUP_MIN_BLOCKS)
 integrate_kernel(const __grid_constant__ DevMech m, const __grid_constant__ IntegratorParams P,
                  const __grid_constant__ CellIO io) {
     using L = Smem<N, G>;
