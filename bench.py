@@ -53,6 +53,11 @@ METRIC = "chem cells/s per flow step, plain FP64 vs gated surrogate @ max|ΔT|<5
 UNIT = "cells/s"
 WORKLOAD_CELLS = {"batched": 1048576, "small": 4096, "large": 262144}
 L2_FLUSH_BYTES = 256 << 20
+# DRAM bytes (read + write) per cell of one integrator launch on the 9-species
+# mechanism: ncu dram__bytes_read.sum + dram__bytes_write.sum of
+# integrate_kernel<10,32> over 5328 cells (profiles/integrator_group_kernel_small.md),
+# divided by the cells; the traffic grows with the cells integrated
+DRAM_BYTES_PER_CELL = {9: 817640.0 / 5328.0}
 
 
 # ----------------------------------------------------------------------------- helpers
@@ -331,7 +336,10 @@ def run_ours(args, ws, rank, local):
             "gpu_launches": args.steps,
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak.value,
                          "unit": "TFLOP/s", "frac": achieved / peak.value,
-                         "traffic": None,
+                         "traffic": (DRAM_BYTES_PER_CELL[nsp] * n if nsp in DRAM_BYTES_PER_CELL
+                                     else None),
+                         "traffic_note": "DRAM bytes per launch, scaled from an ncu capture "
+                                         "of 5328 cells by the cell count",
                          "peak_source": "FP64 FMA probe measured in this run "
                                         "(no FP64 figure in the measured peaks file)",
                          "kernel_ms": kernel_ms, "flops_per_launch": flops_per_launch},
