@@ -302,6 +302,10 @@ def run_ours(args, ws, rank, local):
         sur = surrogate_leg(args, wl, mech, (T0, p0, rho0, Y0), dt, fp64_ref,
                             ms_local / args.steps, flush, rank)
 
+    props = None
+    if name == "large":
+        props = properties_leg(mech, (T0, p0, rho0, Y0), flush, args.prop_cells)
+
     # FP64 peak on this GPU
     peak = C.c_double(0.0)
     _capi.check(lib.hc_probe_fp64_peak(1 << 16, C.byref(peak), C.c_void_p(stream.cuda_stream)),
@@ -347,11 +351,56 @@ def run_ours(args, ws, rank, local):
             "clocks": clk,
             "cpu_baseline": cpu,
             "surrogate": sur,
+            "properties": props,
         }
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return out
+
+
+def hbm_peak_gbs():
+    """Measured HBM copy bandwidth of this pool's B200s, else the fallback."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def properties_leg(mech, fields0, flush, prop_cells):
+    """Mixture properties (h_i, cp, mu, kappa, D_i) of the workload's cells
+    tiled to prop_cells cells: one properties_kernel launch, timed with CUDA
+    events after an L2 flush; algorithmic bytes = inputs T, p, Y and outputs
+    h_i, D_i, cp, mu, kappa (8 B each)."""
+    import torch
+    T0, p0, _, Y0 = fields0
+    n0 = int(T0.shape[0])
+    reps = max(1, prop_cells // n0)
+    T = T0.repeat(reps).contiguous()
+    p = p0.repeat(reps).contiguous()
+    Y = Y0.repeat(1, reps).contiguous()
+    n, nsp = int(T.shape[0]), int(Y.shape[0])
+    stream = torch.cuda.current_stream()
+    for _ in range(3):
+        mech.properties(T, p, Y)
+    times = []
+    for k in range(5):
+        flush.fill_(float(k))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        mech.properties(T, p, Y)
+        b.record(stream)
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+    ms = float(np.median(times))
+    nbytes = n * 8.0 * ((2 + nsp) + (2 * nsp + 3))
+    peak, src = hbm_peak_gbs()
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    return {"cells": n, "ms": ms, "cells_per_s": n / (ms * 1e-3), "bound": "hbm",
+            "achieved_GBs": gbs, "peak_GBs": peak, "peak_source": src, "frac": gbs / peak,
+            "bytes_per_launch": nbytes}
 
 
 def surrogate_leg(args, wl, mech, fields0, dt, fp64_ref, plain_ms, flush, rank):
@@ -485,6 +534,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--prop-cells", type=int, default=262144,
+                    help="cells of the property leg (large workload)")
     ap.add_argument("--surrogate", type=int, default=1,
                     help="1: also train and time the gated surrogate (batched workload)")
     ap.add_argument("--sur-samples", type=int, default=524288)
