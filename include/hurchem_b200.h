@@ -261,6 +261,19 @@ int hc_source_terms(hc_mech_t mech, int64_t n, const double *T, const double *p,
                     const double *Y, double *Ri, void *stream);
 
 /*
+ * Point-implicit source terms for the flow solver's species equations
+ * (chemistrySource::calculateSourceTermsImp with its default
+ * withoutLastSpec = true, chemistrySource.cpp:1412-1450, via omegaCoupled,
+ * :422-480): Ri[nsp*n] = omega_i W_i [kg/m^3/s] and diag[(nsp-1)*n], the
+ * diagonal of the source Jacobian of the first nsp - 1 species with the last
+ * species' concentration eliminated at fixed density and the temperature
+ * coupling at constant internal energy (the reference's diagSource()).
+ */
+int hc_source_terms_imp(hc_mech_t mech, int64_t n, const double *T, const double *p,
+                        const double *rho, const double *Y, double *Ri, double *diag,
+                        void *stream);
+
+/*
  * Mixture properties (thermoList / transportList, kinetic theory + Wilke):
  * T, p, Y -> ha[nsp*n] (J/kg per species), cp[n] (J/kg/K), mu[n] (Pa s),
  * kappa[n] (W/m/K), D[nsp*n] (m^2/s mixture-averaged). Any output may be NULL.

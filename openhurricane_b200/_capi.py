@@ -88,6 +88,7 @@ SIGNATURES = {
     "hc_rhs_jacobian": (C.c_int, [_VP, C.c_int64] + [_VP] * 5 + [_VP]),
     "hc_source_terms": (C.c_int, [_VP, C.c_int64] + [_VP] * 5 + [_VP]),
     "hc_properties": (C.c_int, [_VP, C.c_int64] + [_VP] * 8 + [_VP]),
+    "hc_source_terms_imp": (C.c_int, [_VP, C.c_int64] + [_VP] * 6 + [_VP]),
     "hc_source_terms_host": (C.c_int, [_VP, C.c_int64] + [_VP] * 5 + [_VP]),
     "hc_properties_host": (C.c_int, [_VP, C.c_int64] + [_VP] * 8 + [_VP]),
     "hc_probe_fp64_peak": (C.c_int, [C.c_int, _VP, _VP]),

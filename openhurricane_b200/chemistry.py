@@ -94,6 +94,19 @@ class Mechanism:
         _capi.check(rc, "hc_source_terms")
         return Ri
 
+    def source_terms_imp(self, T, p, rho, Y, stream=None):
+        """(Ri [nsp, n], diag [nsp-1, n]): source terms and the diagonal source
+        Jacobian of chemistrySource::calculateSourceTermsImp."""
+        n = T.shape[0]
+        Ri = torch.empty_like(Y)
+        diag = torch.empty((self.nsp - 1, n), dtype=torch.float64, device=T.device)
+        rc = _capi.load().hc_source_terms_imp(self.handle, n, _ptr(_f64(T, "T")),
+                                              _ptr(_f64(p, "p")), _ptr(_f64(rho, "rho")),
+                                              _ptr(_f64(Y, "Y")), _ptr(Ri), _ptr(diag),
+                                              _stream(stream))
+        _capi.check(rc, "hc_source_terms_imp")
+        return Ri, diag
+
     def properties(self, T, p, Y, stream=None) -> Dict[str, torch.Tensor]:
         """ha [nsp,n] J/kg, cp [n] J/kg/K, mu [n] Pa s, kappa [n] W/m/K, D [nsp,n] m^2/s."""
         n = T.shape[0]
@@ -205,6 +218,16 @@ class ChemistrySource:
                 self._integrate(dt, dt_factor, f.T, f.rho, f.Y, None, False)
         torch.cuda.current_stream().wait_stream(side)
         return g
+
+    def calculateSourceTermsImp(self, withoutLastSpec: bool = True):
+        """Ri and the diagonal source Jacobian (chemistrySource::calculateSourceTermsImp);
+        the diagonal is returned for the first nsp - 1 species, the form the
+        flow solver's coupled solve uses (withoutLastSpec = true)."""
+        if not withoutLastSpec:
+            raise NotImplementedError("only the withoutLastSpec = true form is built")
+        f = self.flow
+        self._Ri, self.diagSource = self.mech.source_terms_imp(f.T, f.p, f.rho, f.Y)
+        return self._Ri, self.diagSource
 
     def calculateSourceTerms(self, withoutLastSpec: bool = False):
         """Ri = omega_i W_i at the current state (chemistrySource::calculateSourceTerms)."""

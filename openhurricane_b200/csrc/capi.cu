@@ -716,6 +716,17 @@ int hc_source_terms(hc_mech_t m, int64_t n, const double *T, const double *p, co
     HC_DISPATCH(m, source, m->dm, n, T, p, rho, Y, Ri, st, g_err);
 }
 
+int hc_source_terms_imp(hc_mech_t m, int64_t n, const double *T, const double *p,
+                        const double *rho, const double *Y, double *Ri, double *diag,
+                        void *stream) {
+    if (!m) return fail(HC_E_INVALID, "null mechanism");
+    if (n <= 0) return HC_OK;
+    if (!T || !p || !rho || !Y || !Ri || !diag) return fail(HC_E_INVALID, "null field");
+    if (m->dm.nsp < 2) return fail(HC_E_INVALID, "point-implicit terms need at least 2 species");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    HC_DISPATCH(m, srcimp, m->dm, n, T, p, rho, Y, Ri, diag, st, g_err);
+}
+
 int hc_properties(hc_mech_t m, int64_t n, const double *T, const double *p, const double *Y,
                   double *ha, double *cp, double *mu, double *kappa, double *D, void *stream) {
     if (!m) return fail(HC_E_INVALID, "null mechanism");

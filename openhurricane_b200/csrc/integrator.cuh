@@ -790,4 +790,51 @@ source_kernel(const __grid_constant__ DevMech m, int64_t n, const double *T, con
     if (lane < nsp) Ri[(int64_t)lane * n + k] = f * ldg(&m.W[lane]);
 }
 
+// point-implicit source terms (chemistrySource::calculateSourceTermsImp with
+// withoutLastSpec = true, chemistrySource.cpp:1412-1450, via omegaCoupled,
+// :422-480): Ri_i = omega_i W_i for every species and, for j < nsp - 1,
+//   diag_j = J_jj - (W_j / W_L) J_jL + J_jT W_j (e_L - e_j) / (rho c_v)
+// with L the last species (c_L follows from the others at fixed density,
+// reactionTypes.cpp:761-832), e_i = h_i - R_i T (thermo.inl:168-171) and
+// c_v = c_p - R_mix (thermoList.inl:145-149)
+template <int N, int G>
+__global__ void __launch_bounds__(128)
+source_imp_kernel(const __grid_constant__ DevMech m, int64_t n, const double *T, const double *p,
+                  const double *rho, const double *Y, double *Ri, double *diag) {
+    using L = Smem<N, G>;
+    extern __shared__ double smem_all[];
+    constexpr int CPB = cells_per_block(G);
+    const int gid = threadIdx.x / G;
+    double *s = smem_all + (size_t)gid * L::kSize;
+    const int64_t k = (int64_t)blockIdx.x * CPB + gid;
+    if (k >= n) return;
+    const Group<G> g = make_group<G>(s, gid, L::kRed, L::kRedI);
+    CellCtx<N, G> ctx(m, kNoParams, g, s);
+    ctx.p = p[k];
+    const int nsp = m.nsp, lane = g.lane, Ls = nsp - 1;
+    const double W = (lane < nsp) ? ldg(&m.W[lane]) : 1.0;
+    const double Yi = (lane < nsp) ? Y[(int64_t)lane * n + k] : 0.0;
+    const double Tk = T[k], rk = rho[k];
+    double y = 0.0;
+    if (lane < nsp) y = rk * Yi / W;
+    if (lane == nsp) y = Tk;
+    const double f = ctx.evaluate(y, true);
+    if (lane < nsp) Ri[(int64_t)lane * n + k] = f * W;
+    double cpi = 0.0, hi = 0.0;
+    if (lane < nsp) species_cp_h(m, lane, Tk, cpi, hi);
+    const double cp_mix = g.sum(Yi * cpi);
+    const double ymw = g.sum((lane < nsp) ? Yi / W : 0.0);
+    const double cv = cp_mix - kRu * ymw;
+    const double ei = hi - (kRu / W) * Tk;
+    if (lane == Ls) s[L::kMisc + 5] = ei;
+    g.sync();
+    const double eL = s[L::kMisc + 5];
+    if (lane < Ls) {
+        const double *row = &s[L::kJ + lane * L::LD];
+        const double WL = ldg(&m.W[Ls]);
+        diag[(int64_t)lane * n + k] =
+            row[lane] - (W / WL) * row[Ls] + row[nsp] * W * (eL - ei) / (rk * cv);
+    }
+}
+
 }  // namespace hc

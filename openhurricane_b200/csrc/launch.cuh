@@ -69,6 +69,19 @@ struct Launch {
         HC_LCUDA(cudaGetLastError());
         return HC_OK;
     }
+
+    static int srcimp(const DevMech &m, int64_t n, const double *T, const double *p,
+                      const double *rho, const double *Y, double *Ri, double *diag,
+                      cudaStream_t st, std::string &err) {
+        auto kern = source_imp_kernel<N, G>;
+        const size_t sm = smem_bytes();
+        HC_LCUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        const int64_t grid = (n + kCellsPerBlock - 1) / kCellsPerBlock;
+        if (grid <= 0) return HC_OK;
+        kern<<<(unsigned)grid, G * kCellsPerBlock, sm, st>>>(m, n, T, p, rho, Y, Ri, diag);
+        HC_LCUDA(cudaGetLastError());
+        return HC_OK;
+    }
 };
 
 }  // namespace hc
@@ -87,4 +100,9 @@ struct Launch {
                            const double *rho, const double *Y, double *Ri, cudaStream_t st,     \
                            std::string &err) {                                                  \
         return hc::Launch<N, G>::source(m, n, T, p, rho, Y, Ri, st, err);                       \
+    }                                                                                           \
+    int variant_srcimp_##S(const hc::DevMech &m, int64_t n, const double *T, const double *p,   \
+                           const double *rho, const double *Y, double *Ri, double *diag,        \
+                           cudaStream_t st, std::string &err) {                                 \
+        return hc::Launch<N, G>::srcimp(m, n, T, p, rho, Y, Ri, diag, st, err);                 \
     }

@@ -19,7 +19,10 @@
                            std::string &err);                                                   \
     int variant_source_##S(const hc::DevMech &m, int64_t n, const double *T, const double *p,   \
                            const double *rho, const double *Y, double *Ri, cudaStream_t st,     \
-                           std::string &err);
+                           std::string &err);                                                   \
+    int variant_srcimp_##S(const hc::DevMech &m, int64_t n, const double *T, const double *p,   \
+                           const double *rho, const double *Y, double *Ri, double *diag,        \
+                           cudaStream_t st, std::string &err);
 
 HC_DECLARE_VARIANT(10)
 HC_DECLARE_VARIANT(16)

@@ -27,6 +27,12 @@
 //               and per-reaction kf/Kc values at the state's T.
 //   props     : cells file -> per-species ha_i, mixture cp, mu, kappa and
 //               mixture-averaged D_i (thermoList / transportList).
+//   srcimp    : cells file -> the point-implicit source terms the flow solver
+//               asks for (chemistrySource::calculateSourceTermsImp with its
+//               default withoutLastSpec = true, chemistrySource.cpp:1412-1450):
+//               Ri = omega_i W_i for every species and the diagonal source
+//               Jacobian of the first nsp - 1 species, from omegaCoupled
+//               (chemistrySource.cpp:422-480) at the cell's state.
 //
 // Binary formats (little endian, all int64 header words then float64):
 //   cells  : nsp, n, T[n], p[n], rho[n], dt[n], subDt0[n], Y[nsp*n] (species-major)
@@ -35,6 +41,7 @@
 //   katout : nsp, nrc, n, per state: dydt[nsp+1], J[(nsp+1)^2] row-major,
 //            per species (cp0, ha0, s0, g0, G0, DG0DT, Dcp_pDT), per reaction (kf, Kc, kr)
 //   props  : nsp, n, per cell: ha[nsp], cp, mu, kappa, D[nsp]
+//   srcimp : nsp, n, per cell: Ri[nsp], diag[nsp-1]
 
 #include "commonInclude.hpp"
 #include "dataStructure.hpp"
@@ -77,6 +84,8 @@ const char *envOr(const char *k, const char *d) {
 class OracleChem : public ODESolver<chemistrySource> {
 public:
     OracleChem(flowModel &flows, const controller &cont) : ODESolver<chemistrySource>(flows, cont) {}
+
+    double W(integer i) const { return species_.W(i); }
 
     // One cell of chemistrySource::solve(dt, dtFactor) (chemistrySource.cpp:1511-1555),
     // dtFactor = 1, returning the final concentrations as well as the
@@ -243,6 +252,32 @@ static int runProps(flowModel &flows) {
     return 0;
 }
 
+static int runSrcImp(OracleChem &chem) {
+    std::ifstream fin(envOr("HC_IN", "cells.bin"), std::ios::binary);
+    int64_t hdr[2];
+    fin.read(reinterpret_cast<char *>(hdr), sizeof(hdr));
+    const int64_t nsp = hdr[0], n = hdr[1];
+    auto T = readDoubles(fin, n), p = readDoubles(fin, n), rho = readDoubles(fin, n);
+    auto dt = readDoubles(fin, n), sub0 = readDoubles(fin, n), Y = readDoubles(fin, nsp * n);
+    std::ofstream fout(envOr("HC_OUT", "srcimp.bin"), std::ios::binary);
+    int64_t oh[2] = {nsp, n};
+    fout.write(reinterpret_cast<const char *>(oh), sizeof(oh));
+    realArray yi(nsp), ci(nsp), w(nsp), diag(nsp);
+    std::vector<double> out;
+    out.reserve((2 * nsp - 1) * n);
+    for (int64_t k = 0; k < n; ++k) {
+        for (int64_t i = 0; i < nsp; ++i) {
+            yi[i] = Y[i * n + k];
+            ci[i] = rho[k] * yi[i] / chem.W(i);
+        }
+        chem.omegaCoupled(rho[k], p[k], T[k], ci, yi, w, diag);
+        for (int64_t i = 0; i < nsp; ++i) out.push_back(w[i] * chem.W(i));
+        for (int64_t i = 0; i + 1 < nsp; ++i) out.push_back(diag[i]);
+    }
+    writeDoubles(fout, out);
+    return 0;
+}
+
 static void onSegv(int) {
     void *bt[64];
     int n = backtrace(bt, 64);
@@ -280,6 +315,7 @@ int main(int argc, char *argv[]) {
     if (mode == "integrate") rc = runIntegrate(chem);
     else if (mode == "kat") rc = runKat(chem, *flows);
     else if (mode == "props") rc = runProps(*flows);
+    else if (mode == "srcimp") rc = runSrcImp(chem);
     else rc = 3;
     std::fflush(stdout);
     std::fflush(stderr);

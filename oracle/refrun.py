@@ -217,3 +217,18 @@ def props(case: str, T, p, rho, Y, workdir: Optional[str] = None) -> Dict[str, n
     d = np.fromfile(out, dtype=np.float64, offset=16).reshape(n, 2 * nsp + 3)
     return {"ha": d[:, :nsp].T.copy(), "cp": d[:, nsp].copy(), "mu": d[:, nsp + 1].copy(),
             "kappa": d[:, nsp + 2].copy(), "D": d[:, nsp + 3:].T.copy(), "seconds": secs}
+
+
+def srcimp(case: str, T, p, rho, Y, workdir: Optional[str] = None) -> Dict[str, np.ndarray]:
+    """The reference's point-implicit source terms at the given states:
+    Ri [nsp, n] and the diagonal source Jacobian diag [nsp-1, n]
+    (chemistrySource::calculateSourceTermsImp with withoutLastSpec = true)."""
+    tmp = workdir or tempfile.mkdtemp(prefix="hcsrc_")
+    Y = np.ascontiguousarray(Y, dtype=np.float64)
+    nsp, n = Y.shape
+    cells = os.path.join(tmp, "cells_src.bin")
+    write_cells(cells, T, p, rho, 0.0, 0.0, Y)
+    out = os.path.join(tmp, "srcimp.bin")
+    _run(case, {"HC_MODE": "srcimp", "HC_IN": cells, "HC_OUT": out}, tmp)
+    d = np.fromfile(out, dtype=np.float64, offset=16).reshape(n, 2 * nsp - 1)
+    return {"Ri": d[:, :nsp].T.copy(), "diag": d[:, nsp:].T.copy()}

@@ -66,8 +66,9 @@ def make(name, mech, cells, dt, nkat, prop_cells, out):
     k = refrun.kat(case, p, T, c, workdir=work)
     pcase = os.path.join(work, "case_props.cont")
     refrun.write_case(pcase, *files, {"flowModel": "laminarFlow"})
-    pr = refrun.props(pcase, prop_cells.T, prop_cells.p, synth.mixture_density(W, prop_cells),
-                      prop_cells.Y, workdir=work)
+    prho = synth.mixture_density(W, prop_cells)
+    pr = refrun.props(pcase, prop_cells.T, prop_cells.p, prho, prop_cells.Y, workdir=work)
+    si = refrun.srcimp(case, prop_cells.T, prop_cells.p, prho, prop_cells.Y, workdir=work)
     np.savez_compressed(
         out, sha=files_sha(files), seed=mech.seed, dt=dt,
         in_T=cells.T, in_p=cells.p, in_rho=rho, in_Y=cells.Y,
@@ -79,7 +80,7 @@ def make(name, mech, cells, dt, nkat, prop_cells, out):
         kat_rates=np.stack([k["kf"], k["Kc"], k["kr"]], axis=-1),
         prop_T=prop_cells.T, prop_p=prop_cells.p, prop_Y=prop_cells.Y,
         prop_ha=pr["ha"], prop_cp=pr["cp"], prop_mu=pr["mu"], prop_kappa=pr["kappa"],
-        prop_D=pr["D"])
+        prop_D=pr["D"], prop_rho=prho, srcimp_Ri=si["Ri"], srcimp_diag=si["diag"])
     print(name, "written", out, "reference seconds", res["seconds"])
 
 

@@ -91,3 +91,16 @@ def test_oracle_bit_exact_vs_reference_binary(small):
     for k in ("T", "Y", "rho", "c", "subdt"):
         assert np.array_equal(o[k], r[k]), k
     assert o["status"][0] == 1 and r["status"][0] == 1
+
+
+@pytest.mark.parametrize("name", ["small", "large"])
+def test_point_implicit_oracle_vs_reference_golden(name, small, large):
+    """Ri and the diagonal source Jacobian of calculateSourceTermsImp."""
+    from oracle import srcimp_oracle
+    mk = small if name == "small" else large
+    g = _load(name)
+    o = srcimp_oracle.srcimp(mk["tables"], g["prop_T"], g["prop_p"], g["prop_rho"], g["prop_Y"])
+    assert np.array_equal(o["Ri"], g["srcimp_Ri"])
+    ref = g["srcimp_diag"]
+    scale = np.abs(ref).max(axis=0, keepdims=True)
+    assert (np.abs(o["diag"] - ref) / scale).max() < 1e-14
