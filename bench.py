@@ -254,7 +254,7 @@ def run_ours(args, ws, rank, local):
     kernel_ms = ms_local / args.steps
     clk = clocks.stop()
     # the FP64 result of the last timed step (from the pristine inputs): the
-    # reference the surrogate is judged against
+    # reference the surrogate is compared with
     fp64_ref = (flow.T.clone(), flow.Y.clone())
 
     # end to end: host (pinned) buffers through hc_integrate_host
@@ -406,7 +406,7 @@ def properties_leg(mech, fields0, flush, prop_cells):
 def surrogate_leg(args, wl, mech, fields0, dt, fp64_ref, plain_ms, flush, rank):
     """Train the gated surrogate on samples of the FP64 GPU integrator (states
     of the same distribution, another seed), then time its flow step on the
-    workload's cells and judge it against the FP64 step."""
+    workload's cells and compare it with the FP64 step."""
     import torch
     from openhurricane_b200 import _capi, workloads
     from openhurricane_b200.chemistry import Flow
@@ -476,7 +476,7 @@ def surrogate_leg(args, wl, mech, fields0, dt, fp64_ref, plain_ms, flush, rank):
             "train_samples": n_train, "train_epochs": args.sur_epochs, "batch": 8192,
             "final_loss": losses[-1] if losses else None,
             "sample_gen_s": t_gen, "train_s": t_train,
-            "judge": "FP64 GPU integrator on the same cells (atol 1e-11, rtol 1e-4)"}
+            "compared_with": "FP64 GPU integrator on the same cells (atol 1e-11, rtol 1e-4)"}
 
 
 def run_reference(args, ws, rank):

@@ -659,7 +659,10 @@ template <int N, int G>
 #ifndef HC_GROUP_MIN_BLOCKS
 #define HC_GROUP_MIN_BLOCKS 4   // blocks of 128 threads per SM the 32-lane groups are built for (measured best)
 #endif
-__global__ void __launch_bounds__(128, (G == 64) ? 2 : HC_GROUP_MIN_BLOCKS)
+#ifndef HC_GROUP64_MIN_BLOCKS
+#define HC_GROUP64_MIN_BLOCKS 2   // the same for the 64-lane groups
+#endif
+__global__ void __launch_bounds__(128, (G == 64) ? HC_GROUP64_MIN_BLOCKS : HC_GROUP_MIN_BLOCKS)
 integrate_kernel(const __grid_constant__ DevMech m, const __grid_constant__ IntegratorParams P,
                  const __grid_constant__ CellIO io) {
     using L = Smem<N, G>;

@@ -1,6 +1,6 @@
 """Gated surrogate on the GPU: trained by the library's own BF16 kernels on
 samples of the FP64 GPU integrator, applied through the conservation +
-confidence gate with the FP64 integrator as fallback, and judged against a
+confidence gate with the FP64 integrator as fallback, and compared with a
 plain FP64 integration of the same cells."""
 import numpy as np
 import pytest
