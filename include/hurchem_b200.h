@@ -261,6 +261,17 @@ int hc_source_terms(hc_mech_t mech, int64_t n, const double *T, const double *p,
                     const double *Y, double *Ri, void *stream);
 
 /*
+ * Temperature from the mixture's mass enthalpy at constant pressure
+ * (thermoList::THa_p, thermoList.cpp:501-533, with the reference's step
+ * tolerance 1e-4 T0 and 100-iteration cap): ha[n] J/kg, Y[nsp*n], starting
+ * temperatures T0[n] -> T[n]; flag[n] (optional) = 0 clamped at TLow,
+ * 1 inside, 2 clamped at THigh (the reference's defaults: 50 K, 5000 K).
+ */
+int hc_temperature_from_enthalpy(hc_mech_t mech, int64_t n, const double *ha, const double *Y,
+                                 const double *T0, double TLow, double THigh, double *T,
+                                 int32_t *flag, void *stream);
+
+/*
  * Point-implicit source terms for the flow solver's species equations
  * (chemistrySource::calculateSourceTermsImp with its default
  * withoutLastSpec = true, chemistrySource.cpp:1412-1450, via omegaCoupled,

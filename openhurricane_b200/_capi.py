@@ -89,6 +89,8 @@ SIGNATURES = {
     "hc_source_terms": (C.c_int, [_VP, C.c_int64] + [_VP] * 5 + [_VP]),
     "hc_properties": (C.c_int, [_VP, C.c_int64] + [_VP] * 8 + [_VP]),
     "hc_source_terms_imp": (C.c_int, [_VP, C.c_int64] + [_VP] * 6 + [_VP]),
+    "hc_temperature_from_enthalpy": (C.c_int, [_VP, C.c_int64] + [_VP] * 3 +
+                                     [C.c_double, C.c_double] + [_VP] * 3),
     "hc_source_terms_host": (C.c_int, [_VP, C.c_int64] + [_VP] * 5 + [_VP]),
     "hc_properties_host": (C.c_int, [_VP, C.c_int64] + [_VP] * 8 + [_VP]),
     "hc_probe_fp64_peak": (C.c_int, [C.c_int, _VP, _VP]),

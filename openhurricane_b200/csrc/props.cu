@@ -149,4 +149,64 @@ int launch_properties(const DevMech &m, int64_t n, const double *T, const double
     return HC_OK;
 }
 
+// Temperature from the mixture's mass enthalpy at constant pressure,
+// thermoList::THa_p (thermoList.cpp:501-533): Newton steps
+// T <- limit(T - (h(T) - ha) / cp(T)) from T0 until |dT| <= T0 tol, at most
+// max_iter + 1 steps; limit clamps to [TLow, THigh] and sets the flag
+// (0 below, 1 inside, 2 above; thermoList.cpp:152-163). Thread per cell.
+__global__ void t_from_ha_kernel(const __grid_constant__ DevMech m, int64_t n,
+                                 const double *__restrict__ ha, const double *__restrict__ Y,
+                                 const double *__restrict__ T0, double TLow, double THigh,
+                                 double tol, int max_iter, double *__restrict__ Tout,
+                                 int32_t *__restrict__ flag) {
+    const int nsp = m.nsp;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        double Tnew = T0[c];
+        const double Ttol = T0[c] * tol;
+        int it = 0, f = 1;
+        while (true) {
+            const double Test = Tnew;
+            double hm = 0.0, cpm = 0.0;
+            for (int i = 0; i < nsp; ++i) {
+                double cp, h;
+                species_cp_h(m, i, Test, cp, h);
+                const double yi = Y[(int64_t)i * n + c];
+                hm += h * yi;
+                cpm += cp * yi;
+            }
+            const double v = Test - (hm - ha[c]) / cpm;
+            if (v < TLow) {
+                f = 0;
+                Tnew = TLow;
+            } else if (v > THigh) {
+                f = 2;
+                Tnew = THigh;
+            } else {
+                f = 1;
+                Tnew = v;
+            }
+            if (it++ > max_iter) break;
+            if (!(fabs(Tnew - Test) > Ttol)) break;
+        }
+        Tout[c] = Tnew;
+        if (flag) flag[c] = f;
+    }
+}
+
+int launch_t_from_ha(const DevMech &m, int64_t n, const double *ha, const double *Y,
+                     const double *T0, double TLow, double THigh, double *T, int32_t *flag,
+                     cudaStream_t st, std::string &err) {
+    if (n <= 0) return HC_OK;
+    const int64_t blocks = (n + 127) / 128;
+    t_from_ha_kernel<<<(unsigned)(blocks < 148 * 64 ? blocks : 148 * 64), 128, 0, st>>>(
+        m, n, ha, Y, T0, TLow, THigh, 1.0e-4, 100, T, flag);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        err = std::string("t_from_ha_kernel: ") + cudaGetErrorString(e);
+        return HC_E_CUDA;
+    }
+    return HC_OK;
+}
+
 }  // namespace hc

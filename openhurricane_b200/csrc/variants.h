@@ -46,3 +46,8 @@ struct T2Mech;
 int variant_integrate_t2(int N, const hc::T2Mech &m, int num_sms, const hc::IntegratorParams &P,
                          const hc::CellIO &io, double *ylast, int block, cudaStream_t st,
                          std::string &err);
+namespace hc {
+int launch_t_from_ha(const DevMech &m, int64_t n, const double *ha, const double *Y,
+                     const double *T0, double TLow, double THigh, double *T, int32_t *flag,
+                     cudaStream_t st, std::string &err);
+}

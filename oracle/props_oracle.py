@@ -61,3 +61,56 @@ def properties(t, T, p, Y):
         D = np.where(x < 1.0 - 1e-300, (1.0 - x) / s, 0.0)
     D = np.where(np.isinf(D), 0.0, D)
     return {"ha": h, "cp": cpm, "mu": mum, "kappa": kappam, "D": D}
+
+
+def species_cp_h(t, T):
+    """Mass-basis cp_i and h_i [nsp, n] at temperatures T (JANAF.cpp:155-199)."""
+    T = np.asarray(T, float)
+    tl, tc, th = t.Trange[:, 0][:, None], t.Trange[:, 1][:, None], t.Trange[:, 2][:, None]
+    Tb = T[None, :]
+    a = np.where((Tb < tc)[..., None], t.nasa[:, 0, None, :], t.nasa[:, 1, None, :])
+    T0 = np.clip(Tb, tl, th)
+    cp = ((((a[..., 4] * T0 + a[..., 3]) * T0 + a[..., 2]) * T0 + a[..., 1]) * T0 + a[..., 0])
+    h = ((((a[..., 4] / 5.0 * T0 + a[..., 3] / 4.0) * T0 + a[..., 2] / 3.0) * T0
+          + a[..., 1] / 2.0) * T0 + a[..., 0]) * T0 + a[..., 5]
+    h = h + np.where((Tb < tl) | (Tb > th), cp * (Tb - T0), 0.0)
+    return cp, h
+
+
+def temperature_from_ha(t, ha, p, Y, T0, TLow=50.0, THigh=5000.0, tol=1e-4, max_iter=100):
+    """thermoList::THa_p (thermoList.cpp:501-533): Newton on the mixture's
+    mass enthalpy, T <- limit(T - (h(T) - ha) / cp(T)), until |dT| <= T0 tol
+    or more than max_iter iterations; limit clamps to [TLow, THigh] and sets
+    iFlag 0 (below), 1 (inside), 2 (above) (thermoList.cpp:152-163).
+    Cell by cell, in the reference's order of operations."""
+    ha = np.asarray(ha, float)
+    Y = np.asarray(Y, float)
+    T0 = np.asarray(T0, float)
+    n = ha.shape[0]
+    Tout = np.empty(n)
+    flag = np.empty(n, np.int32)
+    for k in range(n):
+        Tnew = T0[k]
+        Ttol = T0[k] * tol
+        it = 0
+        f = 1
+        while True:
+            Test = Tnew
+            cp, h = species_cp_h(t, np.array([Test]))
+            hm = float((h[:, 0] * Y[:, k]).sum())
+            cpm = float((cp[:, 0] * Y[:, k]).sum())
+            v = Test - (hm - ha[k]) / cpm
+            if v < TLow:
+                f, Tnew = 0, TLow
+            elif v > THigh:
+                f, Tnew = 2, THigh
+            else:
+                f, Tnew = 1, v
+            it += 1
+            if it - 1 > max_iter:
+                break
+            if not (abs(Tnew - Test) > Ttol):
+                break
+        Tout[k] = Tnew
+        flag[k] = f
+    return Tout, flag

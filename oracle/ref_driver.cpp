@@ -27,6 +27,10 @@
 //               and per-reaction kf/Kc values at the state's T.
 //   props     : cells file -> per-species ha_i, mixture cp, mu, kappa and
 //               mixture-averaged D_i (thermoList / transportList).
+//   tha       : cells file (dt column = target mass enthalpy ha, subDt0
+//               column = starting temperature T0) -> T from
+//               thermoList::THa_p(ha, p, T0, iFlag, yi) (thermoList.cpp:501-533)
+//               and iFlag per cell.
 //   srcimp    : cells file -> the point-implicit source terms the flow solver
 //               asks for (chemistrySource::calculateSourceTermsImp with its
 //               default withoutLastSpec = true, chemistrySource.cpp:1412-1450):
@@ -42,6 +46,7 @@
 //            per species (cp0, ha0, s0, g0, G0, DG0DT, Dcp_pDT), per reaction (kf, Kc, kr)
 //   props  : nsp, n, per cell: ha[nsp], cp, mu, kappa, D[nsp]
 //   srcimp : nsp, n, per cell: Ri[nsp], diag[nsp-1]
+//   tha    : n, per cell: T, iFlag
 
 #include "commonInclude.hpp"
 #include "dataStructure.hpp"
@@ -252,6 +257,29 @@ static int runProps(flowModel &flows) {
     return 0;
 }
 
+static int runTHa(flowModel &flows) {
+    std::ifstream fin(envOr("HC_IN", "cells.bin"), std::ios::binary);
+    int64_t hdr[2];
+    fin.read(reinterpret_cast<char *>(hdr), sizeof(hdr));
+    const int64_t nsp = hdr[0], n = hdr[1];
+    auto T = readDoubles(fin, n), p = readDoubles(fin, n), rho = readDoubles(fin, n);
+    auto ha = readDoubles(fin, n), T0 = readDoubles(fin, n), Y = readDoubles(fin, nsp * n);
+    const auto &thl = flows.mixtures().thermalTable();
+    std::ofstream fout(envOr("HC_OUT", "tha.bin"), std::ios::binary);
+    int64_t oh[1] = {n};
+    fout.write(reinterpret_cast<const char *>(oh), sizeof(oh));
+    realArray yi(nsp);
+    std::vector<double> out;
+    for (int64_t k = 0; k < n; ++k) {
+        for (int64_t i = 0; i < nsp; ++i) yi[i] = Y[i * n + k];
+        integer flag = 1;
+        out.push_back(thl.THa_p(ha[k], p[k], T0[k], flag, yi));
+        out.push_back((double)flag);
+    }
+    writeDoubles(fout, out);
+    return 0;
+}
+
 static int runSrcImp(OracleChem &chem) {
     std::ifstream fin(envOr("HC_IN", "cells.bin"), std::ios::binary);
     int64_t hdr[2];
@@ -316,6 +344,7 @@ int main(int argc, char *argv[]) {
     else if (mode == "kat") rc = runKat(chem, *flows);
     else if (mode == "props") rc = runProps(*flows);
     else if (mode == "srcimp") rc = runSrcImp(chem);
+    else if (mode == "tha") rc = runTHa(*flows);
     else rc = 3;
     std::fflush(stdout);
     std::fflush(stderr);

@@ -232,3 +232,18 @@ def srcimp(case: str, T, p, rho, Y, workdir: Optional[str] = None) -> Dict[str, 
     _run(case, {"HC_MODE": "srcimp", "HC_IN": cells, "HC_OUT": out}, tmp)
     d = np.fromfile(out, dtype=np.float64, offset=16).reshape(n, 2 * nsp - 1)
     return {"Ri": d[:, :nsp].T.copy(), "diag": d[:, nsp:].T.copy()}
+
+
+def tha(case: str, ha, p, T0, Y, workdir: Optional[str] = None) -> Dict[str, np.ndarray]:
+    """The reference's temperature from mixture enthalpy at constant p
+    (thermoList::THa_p) for each cell, starting from T0; returns T and iFlag."""
+    tmp = workdir or tempfile.mkdtemp(prefix="hctha_")
+    Y = np.ascontiguousarray(Y, dtype=np.float64)
+    nsp, n = Y.shape
+    cells = os.path.join(tmp, "cells_tha.bin")
+    # the cells format carries ha in the dt column and T0 in the subDt0 column
+    write_cells(cells, np.asarray(T0, np.float64), p, np.ones(n), ha, T0, Y)
+    out = os.path.join(tmp, "tha.bin")
+    _run(case, {"HC_MODE": "tha", "HC_IN": cells, "HC_OUT": out}, tmp)
+    d = np.fromfile(out, dtype=np.float64, offset=8).reshape(n, 2)
+    return {"T": d[:, 0].copy(), "iflag": d[:, 1].astype(np.int32)}

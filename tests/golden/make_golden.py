@@ -69,6 +69,12 @@ def make(name, mech, cells, dt, nkat, prop_cells, out):
     prho = synth.mixture_density(W, prop_cells)
     pr = refrun.props(pcase, prop_cells.T, prop_cells.p, prho, prop_cells.Y, workdir=work)
     si = refrun.srcimp(case, prop_cells.T, prop_cells.p, prho, prop_cells.Y, workdir=work)
+    # temperature from enthalpy: the cells' own mass enthalpy, started 300 K
+    # away (and once from far outside the table range)
+    ha = (pr["ha"] * prop_cells.Y).sum(axis=0)     # the reference's per-species ha_i
+    T0 = prop_cells.T + np.where(np.arange(prop_cells.T.shape[0]) % 2 == 0, 300.0, -300.0)
+    T0[0] = 20.0
+    th = refrun.tha(case, ha, prop_cells.p, T0, prop_cells.Y, workdir=work)
     np.savez_compressed(
         out, sha=files_sha(files), seed=mech.seed, dt=dt,
         in_T=cells.T, in_p=cells.p, in_rho=rho, in_Y=cells.Y,
@@ -80,7 +86,8 @@ def make(name, mech, cells, dt, nkat, prop_cells, out):
         kat_rates=np.stack([k["kf"], k["Kc"], k["kr"]], axis=-1),
         prop_T=prop_cells.T, prop_p=prop_cells.p, prop_Y=prop_cells.Y,
         prop_ha=pr["ha"], prop_cp=pr["cp"], prop_mu=pr["mu"], prop_kappa=pr["kappa"],
-        prop_D=pr["D"], prop_rho=prho, srcimp_Ri=si["Ri"], srcimp_diag=si["diag"])
+        prop_D=pr["D"], prop_rho=prho, srcimp_Ri=si["Ri"], srcimp_diag=si["diag"],
+        tha_ha=ha, tha_T0=T0, tha_T=th["T"], tha_flag=th["iflag"])
     print(name, "written", out, "reference seconds", res["seconds"])
 
 

@@ -104,3 +104,17 @@ def test_point_implicit_oracle_vs_reference_golden(name, small, large):
     ref = g["srcimp_diag"]
     scale = np.abs(ref).max(axis=0, keepdims=True)
     assert (np.abs(o["diag"] - ref) / scale).max() < 1e-14
+
+
+@pytest.mark.parametrize("name", ["small", "large"])
+def test_temperature_from_enthalpy_oracle_vs_reference_golden(name, small, large):
+    """thermoList::THa_p: Newton on the mixture enthalpy with the reference's
+    tolerance, iteration cap and [TLow, THigh] clamp."""
+    from oracle import props_oracle
+    mk = small if name == "small" else large
+    g = _load(name)
+    T, flag = props_oracle.temperature_from_ha(mk["tables"], g["tha_ha"], g["prop_p"], g["prop_Y"],
+                                               g["tha_T0"])
+    assert np.array_equal(flag, g["tha_flag"])
+    assert np.abs(T - g["tha_T"]).max() < 1e-9
+    assert flag[0] == 1   # started at 20 K, below TLow: clamped, then converged inside

@@ -328,3 +328,15 @@ def test_point_implicit_source_terms_vs_reference_golden(name, small, large):
     for got, ref in ((Ri.cpu().numpy(), o["Ri"]), (diag.cpu().numpy(), o["diag"])):
         scale = np.abs(ref).max(axis=0, keepdims=True) + 1e-300
         assert (np.abs(got - ref) / scale).max() < 1e-10
+
+
+@pytest.mark.parametrize("name", ["small", "large"])
+def test_temperature_from_enthalpy_vs_reference_golden(name, small, large):
+    mk = small if name == "small" else large
+    g0 = _golden(name)
+    dev = _cuda()
+    m = _mech(mk["tables"])
+    d = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+    T, flag = m.temperature_from_enthalpy(d(g0["tha_ha"]), d(g0["prop_Y"]), d(g0["tha_T0"]))
+    assert np.array_equal(flag.cpu().numpy(), g0["tha_flag"])
+    assert np.abs(T.cpu().numpy() - g0["tha_T"]).max() < 1e-8
