@@ -306,6 +306,55 @@ int hc_properties_host(hc_mech_t mech, int64_t n, const double *T, const double 
                        const double *Y, double *ha, double *cp, double *mu, double *kappa,
                        double *D, void *stream);
 
+/* ------------------------------------------------------------------------
+ * Record-per-cell forms: the buffers of the reference's CUDA path, one
+ * record of nsp + 2 doubles per cell. The records are transposed on the
+ * device into the species-major fields of the entry points above, computed,
+ * and transposed back. p[n] is optional: NULL takes p from the ideal-gas law,
+ * p = rho Ru T sum_i Y_i / W_i, with the record's rho, T and Y. The records
+ * live in the mechanism's workspace while a call is in flight, so calls on
+ * one mechanism are issued on one stream (or synchronised between streams).
+ * Mechanisms of up to 64 species.
+ *
+ * hc_integrate_aos / hc_integrate_aos_host: records [T, Y_0..Y_{nsp-1}, rho]
+ * (calcChemODEsArray, chemistrySource/src/CUDAChemistrySourceODEs.cu:823-858,
+ * called from CUDAChemistrySource.cpp:377-399) integrated over dt[n]
+ * (already multiplied by dtFactor, as the reference's caller does) with the
+ * warm-start sub-steps subdt[n] (in/out), by this library's implicit-Euler
+ * integrator (the same kernels as hc_integrate). On return each record
+ * holds T and either, return_ci != 0, the concentrations
+ * c_i = Y_i rho_new / W_i [kmol/m^3] with the record's own rho left in place
+ * (the reference's returnCi form, from which its caller forms Ri), or the
+ * mass fractions and the new density. status[n] is optional. The _aos form
+ * takes device pointers and is stream-ordered; the _aos_host form takes host
+ * pointers, synchronises, and returns the number of cells with
+ * HC_CELL_UNDERFLOW or HC_CELL_ITER_LIMIT like hc_integrate_host.
+ */
+int hc_integrate_aos(hc_mech_t mech, const hc_opts *opts, int64_t ncells, double *TYiRho,
+                     const double *p, const double *dt, double *subdt, int return_ci,
+                     int32_t *status, void *stream);
+int hc_integrate_aos_host(hc_mech_t mech, const hc_opts *opts, int64_t ncells, double *TYiRho,
+                          const double *p, const double *dt, double *subdt, int return_ci,
+                          int32_t *status, void *stream);
+
+/*
+ * Explicit source terms from records [Y_0..Y_{nsp-1}, rho, T] (getYiRhoT,
+ * CUDAChemistrySource.cpp:73-81) into RRi[cell * nsp + i] [kg/m^3/s]
+ * (calcOnlyChemSourceTermsAsync via CUDAChemistrySource::calculateSourceTermsAsync,
+ * CUDAChemistrySource.cpp:189-198; read back by laminarSpeciesSolverCUDA.cpp:326-330).
+ * hc_source_terms_aos takes device pointers. hc_source_terms_aos_async takes
+ * host pointers and only enqueues the copies and kernels on the stream: it
+ * returns before the results arrive, the caller does its own host work
+ * meanwhile (the reference computes the viscous fluxes) and synchronises the
+ * stream before reading RRi. With pageable host memory the CUDA runtime
+ * performs the copies synchronously, so pinned buffers (cudaHostAlloc, as
+ * the reference allocates them) are what makes the overlap happen.
+ */
+int hc_source_terms_aos(hc_mech_t mech, int64_t n, const double *YiRhoT, const double *p,
+                        double *RRi, void *stream);
+int hc_source_terms_aos_async(hc_mech_t mech, int64_t n, const double *YiRhoT, const double *p,
+                              double *RRi, void *stream);
+
 /*
  * Measurement utility, no reference counterpart: runs an FP64 FMA-throughput
  * probe on the current device (independent FMA chains on every SM) and

@@ -93,6 +93,12 @@ SIGNATURES = {
                                      [C.c_double, C.c_double] + [_VP] * 3),
     "hc_source_terms_host": (C.c_int, [_VP, C.c_int64] + [_VP] * 5 + [_VP]),
     "hc_properties_host": (C.c_int, [_VP, C.c_int64] + [_VP] * 8 + [_VP]),
+    "hc_integrate_aos": (C.c_int, [_VP, C.POINTER(HcOpts), C.c_int64] + [_VP] * 4 +
+                         [C.c_int, _VP, _VP]),
+    "hc_integrate_aos_host": (C.c_int, [_VP, C.POINTER(HcOpts), C.c_int64] + [_VP] * 4 +
+                              [C.c_int, _VP, _VP]),
+    "hc_source_terms_aos": (C.c_int, [_VP, C.c_int64] + [_VP] * 3 + [_VP]),
+    "hc_source_terms_aos_async": (C.c_int, [_VP, C.c_int64] + [_VP] * 3 + [_VP]),
     "hc_probe_fp64_peak": (C.c_int, [C.c_int, _VP, _VP]),
     "hc_mlp_create": (C.c_int, [C.c_int] * 5 + [C.c_uint64, C.POINTER(_VP)]),
     "hc_mlp_destroy": (C.c_int, [_VP]),

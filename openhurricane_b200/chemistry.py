@@ -94,6 +94,36 @@ class Mechanism:
         _capi.check(rc, "hc_source_terms")
         return Ri
 
+    def source_terms_aos(self, YiRhoT, p=None, stream=None) -> torch.Tensor:
+        """RRi [n, nsp] from records [n, nsp+2] = [Y_0..Y_{nsp-1}, rho, T] (the
+        reference's CUDA source-term buffers); p from the ideal-gas law when None."""
+        n = YiRhoT.shape[0]
+        if YiRhoT.dim() != 2 or YiRhoT.shape[1] != self.nsp + 2:
+            raise ValueError("records must be [n, nsp + 2]")
+        RRi = torch.empty((n, self.nsp), dtype=torch.float64, device=YiRhoT.device)
+        rc = _capi.load().hc_source_terms_aos(self.handle, n, _ptr(_f64(YiRhoT, "YiRhoT")),
+                                              _ptr(None if p is None else _f64(p, "p")),
+                                              _ptr(RRi), _stream(stream))
+        _capi.check(rc, "hc_source_terms_aos")
+        return RRi
+
+    def integrate_aos(self, TYiRho, dt, subdt, p=None, return_ci: bool = True, opts=None,
+                      stream=None) -> torch.Tensor:
+        """Integrate records [n, nsp+2] = [T, Y_0..Y_{nsp-1}, rho] in place over
+        dt (the reference's calcChemODEsArray buffers); subdt is updated in
+        place. Returns the per-cell status words."""
+        n = TYiRho.shape[0]
+        if TYiRho.dim() != 2 or TYiRho.shape[1] != self.nsp + 2:
+            raise ValueError("records must be [n, nsp + 2]")
+        st = torch.zeros(n, dtype=torch.int32, device=TYiRho.device)
+        o = opts if opts is not None else _capi.default_opts()
+        rc = _capi.load().hc_integrate_aos(self.handle, C.byref(o), n, _ptr(_f64(TYiRho, "TYiRho")),
+                                           _ptr(None if p is None else _f64(p, "p")),
+                                           _ptr(_f64(dt, "dt")), _ptr(_f64(subdt, "subdt")),
+                                           1 if return_ci else 0, _ptr(st), _stream(stream))
+        _capi.check(rc, "hc_integrate_aos")
+        return st
+
     def source_terms_imp(self, T, p, rho, Y, stream=None):
         """(Ri [nsp, n], diag [nsp-1, n]): source terms and the diagonal source
         Jacobian of chemistrySource::calculateSourceTermsImp."""

@@ -863,6 +863,209 @@ int hc_surrogate_gate(hc_mech_t m, int64_t n, double *T, const double *p, double
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
+// Record-per-cell entry points: the reference's CUDA-path buffers.
+//
+// Integration records are [T, Y_0..Y_{nsp-1}, rho] (calcChemODEsArray,
+// CUDAChemistrySourceODEs.cu:823-858); source-term records are
+// [Y_0..Y_{nsp-1}, rho, T] with RRi[cell * nsp + i] out
+// (calcOnlyChemSourceTermsAsync via CUDAChemistrySource.cpp:189-198). The
+// records are transposed into species-major rows in the mechanism's
+// workspace (rows [T][Y][rho] or [Y][rho][T], so that a transpose of the
+// whole record matrix is all it takes), the species-major kernels run on
+// them, and the results are transposed back. p is taken from the caller when
+// given, else from the ideal-gas law with the record's rho, T and Y.
+// ---------------------------------------------------------------------------
+namespace {
+
+// workspace for the record-per-cell entry points (callers hold m->mu)
+struct AosWs {
+    double *recs;   // device copy of the caller's records (host entry points)
+    double *rows;   // [rec][n]
+    double *p;      // [n]
+    double *dt, *subdt;
+    double *out;    // source terms: Ri rows [nsp][n], then RRi records [n][nsp]
+    int32_t *status;
+};
+
+int aos_ws(hc_mech_t m, int64_t ncells, bool host, bool source, cudaStream_t st, AosWs &w) {
+    const size_t n = (size_t)ncells, rec = (size_t)m->dm.nsp + 2, nsp = (size_t)m->dm.nsp;
+    size_t doubles = n * rec + n;                           // rows, p
+    if (host) doubles += n * rec + (source ? 0 : 2 * n);    // records, dt, subdt
+    if (source) doubles += 2 * n * nsp;                     // Ri rows, RRi records
+    const size_t bytes = sizeof(double) * doubles + sizeof(int32_t) * n + 256;
+    int rc = ensure_ws(m, bytes, st);
+    if (rc != HC_OK) return rc;
+    double *q = static_cast<double *>(m->ws);
+    w = AosWs{};
+    w.rows = q;
+    q += n * rec;
+    w.p = q;
+    q += n;
+    if (host) {
+        w.recs = q;
+        q += n * rec;
+        if (!source) {
+            w.dt = q;
+            q += n;
+            w.subdt = q;
+            q += n;
+        }
+    }
+    if (source) {
+        w.out = q;
+        q += 2 * n * nsp;
+    }
+    w.status = reinterpret_cast<int32_t *>(q);
+    return HC_OK;
+}
+
+// device records in, device records out (stream-ordered)
+int integrate_records(hc_mech_t m, const hc_opts *opts, int64_t n, double *recs, const double *p,
+                      const double *dt, double *subdt, int return_ci, int32_t *status,
+                      const AosWs &w, cudaStream_t st) {
+    const int nsp = m->dm.nsp, rec = nsp + 2;
+    double *T = w.rows, *Y = w.rows + n, *rho = w.rows + (size_t)n * (nsp + 1);
+    int rc = launch_records_to_rows(n, rec, recs, w.rows, st, g_err);
+    if (rc != HC_OK) return rc;
+    if (!p) {
+        rc = launch_ideal_gas_p(n, nsp, m->dm.W, T, rho, Y, w.p, st, g_err);
+        if (rc != HC_OK) return rc;
+        p = w.p;
+    }
+    rc = integrate_impl(m, opts, n, T, p, rho, Y, dt, 1.0, subdt, nullptr, status, nullptr,
+                        nullptr, st);
+    if (rc != HC_OK) return rc;
+    // concentrations: T and c_i written, the record's rho kept (the
+    // reference's returnCi form); else T, Y_i and the new rho
+    return launch_rows_to_records(n, rec, return_ci ? nsp + 1 : rec, w.rows, recs,
+                                  return_ci ? m->dm.W : nullptr, nsp, st, g_err);
+}
+
+int source_records(hc_mech_t m, int64_t n, const double *recs, const double *p, double *RRi,
+                   const AosWs &w, cudaStream_t st) {
+    const int nsp = m->dm.nsp, rec = nsp + 2;
+    double *Y = w.rows, *rho = w.rows + (size_t)n * nsp, *T = w.rows + (size_t)n * (nsp + 1);
+    int rc = launch_records_to_rows(n, rec, recs, w.rows, st, g_err);
+    if (rc != HC_OK) return rc;
+    if (!p) {
+        rc = launch_ideal_gas_p(n, nsp, m->dm.W, T, rho, Y, w.p, st, g_err);
+        if (rc != HC_OK) return rc;
+        p = w.p;
+    }
+    rc = hc_source_terms(m, n, T, p, rho, Y, w.out, st);
+    if (rc != HC_OK) return rc;
+    return launch_rows_to_records(n, nsp, nsp, w.out, RRi, nullptr, nsp, st, g_err);
+}
+
+int aos_zero(hc_mech_t m, const hc_opts *opts, int64_t ncells, cudaStream_t st) {
+    return integrate_impl(m, opts, ncells, nullptr, nullptr, nullptr, nullptr, nullptr, 1.0,
+                          nullptr, nullptr, nullptr, nullptr, nullptr, st);
+}
+
+}  // namespace
+
+extern "C" {
+
+int hc_integrate_aos(hc_mech_t m, const hc_opts *opts, int64_t ncells, double *TYiRho,
+                     const double *p, const double *dt, double *subdt, int return_ci,
+                     int32_t *status, void *stream) {
+    if (!m) return fail(HC_E_INVALID, "null mechanism");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (ncells <= 0) return aos_zero(m, opts, ncells, st);
+    int rc = check_opts(opts);
+    if (rc != HC_OK) return rc;
+    if (!TYiRho || !dt || !subdt) return fail(HC_E_INVALID, "null field");
+    if (m->dm.nsp + 2 > kAosMaxRec) return fail(HC_E_UNSUPPORTED, "too many species for records");
+    std::lock_guard<std::mutex> lk(m->mu);
+    AosWs w;
+    rc = aos_ws(m, ncells, false, false, st, w);
+    if (rc != HC_OK) return rc;
+    return integrate_records(m, opts, ncells, TYiRho, p, dt, subdt, return_ci, status, w, st);
+}
+
+int hc_integrate_aos_host(hc_mech_t m, const hc_opts *opts, int64_t ncells, double *TYiRho,
+                          const double *p, const double *dt, double *subdt, int return_ci,
+                          int32_t *status, void *stream) {
+    if (!m) return fail(HC_E_INVALID, "null mechanism");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (ncells <= 0) return aos_zero(m, opts, ncells, st);
+    int rc = check_opts(opts);
+    if (rc != HC_OK) return rc;
+    if (!TYiRho || !dt || !subdt) return fail(HC_E_INVALID, "null field");
+    if (m->dm.nsp + 2 > kAosMaxRec) return fail(HC_E_UNSUPPORTED, "too many species for records");
+    std::lock_guard<std::mutex> lk(m->mu);
+    AosWs w;
+    rc = aos_ws(m, ncells, true, false, st, w);
+    if (rc != HC_OK) return rc;
+    const size_t n = (size_t)ncells, rec = (size_t)m->dm.nsp + 2;
+    HC_CUDA(cudaMemcpyAsync(w.recs, TYiRho, sizeof(double) * n * rec, cudaMemcpyHostToDevice, st));
+    HC_CUDA(cudaMemcpyAsync(w.dt, dt, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    HC_CUDA(cudaMemcpyAsync(w.subdt, subdt, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    const double *dp = nullptr;
+    if (p) {
+        HC_CUDA(cudaMemcpyAsync(w.p, p, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+        dp = w.p;
+    }
+    rc = integrate_records(m, opts, ncells, w.recs, dp, w.dt, w.subdt, return_ci, w.status, w,
+                           st);
+    if (rc != HC_OK) return rc;
+    HC_CUDA(cudaMemcpyAsync(TYiRho, w.recs, sizeof(double) * n * rec, cudaMemcpyDeviceToHost, st));
+    HC_CUDA(cudaMemcpyAsync(subdt, w.subdt, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    std::vector<int32_t> stat_h;
+    int32_t *stat_out = status;
+    if (!stat_out) {
+        stat_h.resize(n);
+        stat_out = stat_h.data();
+    }
+    HC_CUDA(cudaMemcpyAsync(stat_out, w.status, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
+    HC_CUDA(cudaStreamSynchronize(st));
+    return count_bad_status(stat_out, ncells);
+}
+
+int hc_source_terms_aos(hc_mech_t m, int64_t n, const double *YiRhoT, const double *p,
+                        double *RRi, void *stream) {
+    if (!m) return fail(HC_E_INVALID, "null mechanism");
+    if (n <= 0) return HC_OK;
+    if (!YiRhoT || !RRi) return fail(HC_E_INVALID, "null field");
+    if (m->dm.nsp + 2 > kAosMaxRec) return fail(HC_E_UNSUPPORTED, "too many species for records");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    std::lock_guard<std::mutex> lk(m->mu);
+    AosWs w;
+    int rc = aos_ws(m, n, false, true, st, w);
+    if (rc != HC_OK) return rc;
+    return source_records(m, n, YiRhoT, p, RRi, w, st);
+}
+
+int hc_source_terms_aos_async(hc_mech_t m, int64_t n, const double *YiRhoT, const double *p,
+                              double *RRi, void *stream) {
+    if (!m) return fail(HC_E_INVALID, "null mechanism");
+    if (n <= 0) return HC_OK;
+    if (!YiRhoT || !RRi) return fail(HC_E_INVALID, "null field");
+    if (m->dm.nsp + 2 > kAosMaxRec) return fail(HC_E_UNSUPPORTED, "too many species for records");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    std::lock_guard<std::mutex> lk(m->mu);
+    AosWs w;
+    int rc = aos_ws(m, n, true, true, st, w);
+    if (rc != HC_OK) return rc;
+    const size_t nn = (size_t)n, nsp = (size_t)m->dm.nsp, rec = nsp + 2;
+    HC_CUDA(cudaMemcpyAsync(w.recs, YiRhoT, sizeof(double) * nn * rec, cudaMemcpyHostToDevice, st));
+    const double *dp = nullptr;
+    if (p) {
+        HC_CUDA(cudaMemcpyAsync(w.p, p, sizeof(double) * nn, cudaMemcpyHostToDevice, st));
+        dp = w.p;
+    }
+    double *dR = w.out + nn * nsp;
+    rc = source_records(m, n, w.recs, dp, dR, w, st);
+    if (rc != HC_OK) return rc;
+    // enqueued only: the caller overlaps its own host work and synchronises
+    // the stream before reading RRi
+    HC_CUDA(cudaMemcpyAsync(RRi, dR, sizeof(double) * nn * nsp, cudaMemcpyDeviceToHost, st));
+    return HC_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
 // Allocation-free integration (hc_integrate_noalloc).
 //
 // For callers that must not allocate device memory during the call: a flow

@@ -51,3 +51,14 @@ int launch_t_from_ha(const DevMech &m, int64_t n, const double *ha, const double
                      const double *T0, double TLow, double THigh, double *T, int32_t *flag,
                      cudaStream_t st, std::string &err);
 }
+
+namespace hc {
+// record-per-cell buffers <-> species-major rows (aos.cu)
+constexpr int kAosMaxRec = 66;
+int launch_records_to_rows(int64_t n, int rec, const double *recs, double *rows,
+                           cudaStream_t st, std::string &err);
+int launch_rows_to_records(int64_t n, int rec, int ncols, const double *rows, double *recs,
+                           const double *W, int nsp, cudaStream_t st, std::string &err);
+int launch_ideal_gas_p(int64_t n, int nsp, const double *W, const double *T, const double *rho,
+                       const double *Y, double *p, cudaStream_t st, std::string &err);
+}
