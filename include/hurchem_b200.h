@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define HC_ABI_VERSION 1
+#define HC_ABI_VERSION 2
 
 /* fatal status codes */
 #define HC_OK 0
@@ -54,6 +54,14 @@ extern "C" {
 #define HC_RATE_LINDEMANN 2
 #define HC_RATE_TROE3 3
 #define HC_RATE_TROE4 4
+#define HC_RATE_SRI 5       /* fall-off with the SRI function (fallOffFunctions::SRI) */
+
+/* hc_mech_desc.reversible */
+#define HC_IRREVERSIBLE 0
+#define HC_REVERSIBLE 1         /* kr = kf / Kc (reversibleReactions) */
+#define HC_REVERSIBLE_REV 2     /* kr from explicit reverse Arrhenius parameters, Chemkin REV
+                                   (reversibleReactionWithRevPars); Arrhenius and third-body
+                                   rate laws only, as in the reference */
 
 #define HC_MAX_SIDE 4
 
@@ -71,7 +79,7 @@ typedef struct hc_mech_desc {
     const double *Trange;    /* [nsp*3] Tlow, Tcommon, Thigh */
     const double *nasa;      /* [nsp*14] mass-basis NASA-7: low a0..a6, high a0..a6 */
     const int32_t *rate_type;  /* [nrc] HC_RATE_* */
-    const int32_t *reversible; /* [nrc] 1 reversible, 0 irreversible */
+    const int32_t *reversible; /* [nrc] HC_IRREVERSIBLE, HC_REVERSIBLE or HC_REVERSIBLE_REV */
     const double *arr;       /* [nrc*3] A, beta, Ta (high-pressure limit for fall-off) */
     const double *arr0;      /* [nrc*3] low-pressure limit (fall-off only) */
     const double *troe;      /* [nrc*4] alpha, T***, T*, T** */
@@ -88,6 +96,10 @@ typedef struct hc_mech_desc {
     const int32_t *geom;     /* [nsp] */
     const double *eps_k;     /* [nsp] well depth / kB, K */
     const double *sigma;     /* [nsp] collision diameter, Angstrom */
+    /* since ABI 2; NULL when no reaction uses them */
+    const double *sri;       /* [nrc*5] SRI a, b, c, d, e (HC_RATE_SRI reactions) */
+    const double *arr_rev;   /* [nrc*3] reverse A, beta, Ta (HC_REVERSIBLE_REV reactions; for a
+                                third-body reaction the reverse rate is M times this) */
 } hc_mech_desc;
 
 /*

@@ -191,6 +191,12 @@ static void make_host(const hc_mech_desc *d, HostMech &h) {
     h.bnu = permute(d->bnu, HC_MAX_SIDE);
     h.ford = permute(d->ford, HC_MAX_SIDE);
     h.bord = permute(d->bord, HC_MAX_SIDE);
+    const std::vector<double> zeros5((size_t)nrc * 5, 0.0), zeros3((size_t)nrc * 3, 0.0);
+    h.sri = permute(d->sri ? d->sri : zeros5.data(), 5);
+    h.arr_rev = permute(d->arr_rev ? d->arr_rev : zeros3.data(), 3);
+    h.ext = false;
+    for (int r = 0; r < nrc; ++r)
+        if (d->rate_type[r] == HC_RATE_SRI || d->reversible[r] == HC_REVERSIBLE_REV) h.ext = true;
     h.sum_stoi.assign(nrc, 0.0);
     for (int r = 0; r < nrc; ++r) {
         double s = 0.0;
@@ -202,7 +208,7 @@ static void make_host(const hc_mech_desc *d, HostMech &h) {
 
 // the mechanism in T2Mech form, if it fits the compact kernel's tables
 static bool pack_t2(const HostMech &h, const hc_mech_desc *d, T2Mech &t) {
-    if (h.nsp > kT2MaxSp || h.nrc > kT2MaxRxn) return false;
+    if (h.nsp > kT2MaxSp || h.nrc > kT2MaxRxn || h.ext) return false;
     std::memset(&t, 0, sizeof(t));
     t.nsp = h.nsp;
     t.nrc = h.nrc;
@@ -261,8 +267,19 @@ static int check_desc(const hc_mech_desc *d) {
     for (int r = 0; r < nrc; ++r) {
         if (d->nf[r] < 0 || d->nf[r] > HC_MAX_SIDE || d->nb[r] < 0 || d->nb[r] > HC_MAX_SIDE)
             return fail(HC_E_INVALID, "reaction side larger than HC_MAX_SIDE");
-        if (d->rate_type[r] < 0 || d->rate_type[r] > HC_RATE_TROE4)
+        if (d->rate_type[r] < 0 || d->rate_type[r] > HC_RATE_SRI)
             return fail(HC_E_INVALID, "unknown rate type");
+        if (d->reversible[r] < HC_IRREVERSIBLE || d->reversible[r] > HC_REVERSIBLE_REV)
+            return fail(HC_E_INVALID, "unknown reversibility code");
+        if (d->rate_type[r] == HC_RATE_SRI && !d->sri)
+            return fail(HC_E_INVALID, "SRI reaction without SRI parameters");
+        if (d->reversible[r] == HC_REVERSIBLE_REV) {
+            if (!d->arr_rev) return fail(HC_E_INVALID, "REV reaction without reverse parameters");
+            // reversibleReactionWithRevPars takes Arrhenius and third-body rates only
+            // (chemkinFileRead.cpp:1387-1444)
+            if (d->rate_type[r] != HC_RATE_ARRHENIUS && d->rate_type[r] != HC_RATE_THIRD_BODY)
+                return fail(HC_E_INVALID, "explicit reverse parameters on a fall-off reaction");
+        }
         for (int k = 0; k < d->nf[r]; ++k)
             if (d->fidx[HC_MAX_SIDE * r + k] < 0 || d->fidx[HC_MAX_SIDE * r + k] >= nsp)
                 return fail(HC_E_INVALID, "species index out of range");
@@ -358,6 +375,8 @@ int hc_mech_create(const hc_mech_desc *d, hc_mech_t *out) {
     up(p_arr.data(), 3 * (size_t)nrc, &dm.arr);
     up(p_arr0.data(), 3 * (size_t)nrc, &dm.arr0);
     up(p_troe.data(), 4 * (size_t)nrc, &dm.troe);
+    up(hm.sri.data(), 5 * (size_t)nrc, &dm.sri);
+    up(hm.arr_rev.data(), 3 * (size_t)nrc, &dm.arr_rev);
     up(p_eff.data(), (size_t)nrc * nsp, &dm.eff);
     up(p_nf.data(), nrc, &dm.nf);
     up(p_nb.data(), nrc, &dm.nb);
@@ -460,6 +479,9 @@ int hc_jit_source(const hc_mech_desc *d, int block, char *buf, int64_t cap, int6
         return fail(HC_E_INVALID, "block must be 32, 64 or 128");
     HostMech h;
     make_host(d, h);
+    if (h.ext)
+        return fail(HC_E_UNSUPPORTED,
+                    "no generated kernel for SRI or explicit reverse (REV) rate laws");
     const std::string src = jit_t1_source(h, block);
     *len = (int64_t)src.size();
     if (buf && cap > 0) {
@@ -518,14 +540,15 @@ static int integrate_impl(hc_mech_t m, const hc_opts *opts, int64_t ncells, doub
     io.queue_head = m->queue;
     io.counters = m->queue + 1;
     const int N = m->dm.nsp + 1;
-    const bool t1_ok = N <= 16 && !opts->auto_update_jacobian;
+    const bool t1_ok = N <= 16 && !opts->auto_update_jacobian && !m->host.ext;
     if (m->kernel == 1 && !t1_ok)
         return fail(HC_E_UNSUPPORTED,
-                    "thread-per-cell kernel needs nsp <= 15 and autoUpdateJacobian off");
+                    "thread-per-cell kernel needs nsp <= 15, autoUpdateJacobian off and no SRI "
+                    "or explicit reverse (REV) rate laws");
     if (m->kernel == 4 && !(t1_ok && m->t2_ok))
         return fail(HC_E_UNSUPPORTED,
-                    "compact thread-per-cell kernel needs nsp <= 15, <= 64 reactions and "
-                    "autoUpdateJacobian off");
+                    "compact thread-per-cell kernel needs nsp <= 15, <= 64 reactions, "
+                    "autoUpdateJacobian off and no SRI or explicit reverse (REV) rate laws");
     // automatic choice: the cell group. Per-cell costs in a flow step differ
     // by orders of magnitude, and the step lasts as long as its stiffest
     // cell; the cell group's lanes share each Newton iteration's work and
@@ -548,7 +571,8 @@ static int integrate_impl(hc_mech_t m, const hc_opts *opts, int64_t ncells, doub
     }
     if (m->kernel == 3 && !t1_ok)
         return fail(HC_E_UNSUPPORTED,
-                    "generated thread-per-cell kernel needs nsp <= 15 and autoUpdateJacobian off");
+                    "generated thread-per-cell kernel needs nsp <= 15, autoUpdateJacobian off and "
+                    "no SRI or explicit reverse (REV) rate laws");
     bool use_jit = t1_ok && m->kernel == 3;
     if (use_jit && !m->jit_tried) {
         // first use: generate, compile and load (host work, no stream operation)
@@ -1115,7 +1139,8 @@ extern "C" int hc_integrate_noalloc(hc_mech_t m, const hc_opts *opts, int64_t nc
     const int N = m->dm.nsp + 1;
     if (N > 16 || opts->auto_update_jacobian || !m->t2_ok)
         return fail(HC_E_UNSUPPORTED,
-                    "hc_integrate_noalloc needs nsp <= 15, <= 64 reactions and autoUpdateJacobian off");
+                    "hc_integrate_noalloc needs nsp <= 15, <= 64 reactions, autoUpdateJacobian off "
+                    "and no SRI or explicit reverse (REV) rate laws");
     int dev = -1;
     HC_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 256) return fail(HC_E_CUDA, "device ordinal out of range");

@@ -190,13 +190,23 @@ struct CellCtx {
             k0 = arrK_log(A0, b0, Ta0, T, logT);
             kinf = arrK_log(A, b, Ta, T, logT);
             Pr = k0 / notZeroD(kinf) * M;
-            if (type != kLindemann) lf = troe_logfcent(&m.troe[4 * r], type == kTroe4, T);
-            F = fall_F(type, lf, Pr);
+            if (type == kSRI) {
+                F = sri_F_global(&m.sri[5 * r], T, Pr);
+            } else {
+                if (type != kLindemann) lf = troe_logfcent(&m.troe[4 * r], type == kTroe4, T);
+                F = fall_F(type, lf, Pr);
+            }
             kf = kinf * (Pr / (1.0 + Pr)) * F;
         }
         double kr = 0.0, Kc = 0.0, DKcDT = 0.0;
-        const bool rev = ldg(&m.reversible[r]) != 0;
-        if (rev) {
+        const int rev_kind = ldg(&m.reversible[r]);
+        const bool rev = rev_kind != 0;
+        if (rev_kind == kRevExplicit) {
+            // reversibleReactionWithRevPars::kr (reversibleReactionWithRevPars.hpp:68-76):
+            // the reverse rate law of the same kind, M times it for third-body
+            kr = arr_global(&m.arr_rev[3 * r], T, logT);
+            if (type == kThirdBody) kr = M * kr;
+        } else if (rev) {
             const double *sg = s;
             const EquilK eq = equilibrium(
                 m, r, T, [sg](int i) { return sg[L::kG0 + i]; },
@@ -271,7 +281,10 @@ struct CellCtx {
         } else {
             dkfdT = (Pr / (1.0 + Pr)) * F * (kinf * invT * (b + Ta * invT));
         }
-        double dkrdT = rev ? (dkfdT - kr * DKcDT) / hmax(Kc, kVeryTiny) : 0.0;
+        double dkrdT = 0.0;
+        if (rev_kind == kRevExplicit)
+            dkrdT = kr * invT * (ldg(&m.arr_rev[3 * r + 1]) + ldg(&m.arr_rev[3 * r + 2]) * invT);
+        else if (rev) dkrdT = (dkfdT - kr * DKcDT) / hmax(Kc, kVeryTiny);
 #pragma unroll
         for (int k = 0; k < kMaxSide; ++k) {
             if (k < nf) dkfdT *= pf[k];
@@ -292,12 +305,17 @@ struct CellCtx {
             if (M > kTiny) {
                 // unimolecularFallOffRR::gamDGamDT (unimolecularFallOffRR.cpp:55-91)
                 const double Pr2 = k0 * M / notZeroD(kinf);
-                const double F2 = fall_F(type, lf, Pr2);
+                const double F2 =
+                    (type == kSRI) ? sri_F_global(&m.sri[5 * r], T, Pr2) : fall_F(type, lf, Pr2);
                 const double dPrdT = Pr2 * ((k0 * invT * (b0 + Ta0 * invT)) / notZeroD(k0) -
                                             (kinf * invT * (b + Ta * invT)) / notZeroD(kinf));
-                const double dFdT = troe_dfdt(type, &m.troe[4 * r], T, Pr2, F2, dPrdT);
+                const double dFdT = (type == kSRI)
+                                        ? sri_dfdt_global(&m.sri[5 * r], T, Pr2, F2, dPrdT)
+                                        : troe_dfdt(type, &m.troe[4 * r], T, Pr2, F2, dPrdT);
                 dgdT = q * (dPrdT / (Pr2 * (1 + Pr2)) + dFdT / F2);
-                const double fabc = troe_dfdci_factor(type, lf, Pr2, F2);
+                const double fabc = (type == kSRI)
+                                        ? sri_dfdci_factor_global(&m.sri[5 * r], T, Pr2, F2)
+                                        : troe_dfdci_factor(type, lf, Pr2, F2);
                 const double g = q * (k0 / notZeroD(kinf)) *
                                  (1.0 / (Pr2 * (1 + Pr2)) + fabc * (1.0 / Pr2) / F2);
                 kind = finite(g) ? 2.0 : 3.0;

@@ -18,6 +18,10 @@ struct HostMech {
     std::vector<double> W, Trange, nasa;
     std::vector<int32_t> rate_type, reversible, nf, nb, fidx, bidx;
     std::vector<double> arr, arr0, troe, eff, fnu, bnu, ford, bord, sum_stoi;
+    std::vector<double> sri, arr_rev;
+    // the mechanism uses rate forms only the cell-group kernels evaluate
+    // (SRI fall-off, explicit reverse parameters)
+    bool ext = false;
 };
 
 struct JitKernel {

@@ -19,6 +19,7 @@ struct DevMech {
     const double *nasa;     // [nsp*14] low a0..a6, high a0..a6 (mass basis)
     const int32_t *rate_type, *reversible;
     const double *arr, *arr0, *troe;  // [nrc*3], [nrc*3], [nrc*4]
+    const double *sri, *arr_rev;      // [nrc*5] SRI a..e, [nrc*3] explicit reverse Arrhenius
     const double *eff;      // [nrc*nsp]
     const int32_t *nf, *nb; // [nrc]
     const int32_t *fidx, *bidx;       // [nrc*4]
@@ -97,6 +98,31 @@ __device__ __forceinline__ void species_cp_h(const DevMech &m, int i, double T, 
     cp = ((((a4 * T0 + a3) * T0 + a2) * T0 + a1) * T0 + a0);
     h = ((((a4 / 5.0 * T0 + a3 / 4.0) * T0 + a2 / 3.0) * T0 + a1 / 2.0) * T0 + a0) * T0 + a5;
     if (out) h += cp * (T - T0);
+}
+
+// Rate forms that only some mechanisms use (SRI fall-off, explicit reverse
+// Arrhenius parameters), kept out of line so that the integrator's register
+// allocation for the common forms does not carry them; parameters are read
+// from the global tables.
+static __device__ __noinline__ double sri_F_global(const double *s, double T, double Pr) {
+    const double p[5] = {ldg(&s[0]), ldg(&s[1]), ldg(&s[2]), ldg(&s[3]), ldg(&s[4])};
+    return sri_F(p, T, Pr);
+}
+
+static __device__ __noinline__ double sri_dfdt_global(const double *s, double T, double Pr, double F,
+                                               double DPrDT) {
+    const double p[5] = {ldg(&s[0]), ldg(&s[1]), ldg(&s[2]), ldg(&s[3]), ldg(&s[4])};
+    return sri_dfdt(p, T, Pr, F, DPrDT);
+}
+
+static __device__ __noinline__ double sri_dfdci_factor_global(const double *s, double T, double Pr,
+                                                       double F) {
+    const double p[5] = {ldg(&s[0]), ldg(&s[1]), ldg(&s[2]), ldg(&s[3]), ldg(&s[4])};
+    return sri_dfdci_factor(p, T, Pr, F);
+}
+
+static __device__ __noinline__ double arr_global(const double *a, double T, double logT) {
+    return arrK_log(ldg(&a[0]), ldg(&a[1]), ldg(&a[2]), T, logT);
 }
 
 __device__ __forceinline__ double troe_logfcent(const double *tr, bool four, double T) {

@@ -25,7 +25,11 @@ constexpr double kPatm = 1.01325e5;        // physicalConstant.hpp:186
 constexpr double kRu = (1.380649e-23 * 6.02214076e23) * 1e3;
 constexpr int kMaxSide = 4;
 
-enum RateType : int32_t { kArrhenius = 0, kThirdBody = 1, kLindemann = 2, kTroe3 = 3, kTroe4 = 4 };
+enum RateType : int32_t {
+    kArrhenius = 0, kThirdBody = 1, kLindemann = 2, kTroe3 = 3, kTroe4 = 4, kSRI = 5
+};
+// reversible flags: 1 kr = kf / Kc, 2 kr from explicit reverse Arrhenius parameters
+constexpr int32_t kRevExplicit = 2;
 
 __device__ __forceinline__ double hmax(double a, double b) { return (a < b) ? b : a; }
 __device__ __forceinline__ double hmin(double a, double b) { return (b < a) ? b : a; }
@@ -123,6 +127,40 @@ __device__ __forceinline__ double troe_dfdt_p(int type, double alpha, double Tss
         2.0 * logPrpc / (nm * nm) * ((dlogPrDT + DcDT) - logPrpc / nm * (DnDT - d * (dlogPrDT + DcDT)));
     const double s1 = 1.0 + inv * inv;
     return (F * ln10 * (DlogFcentDT / s1 - logFcent / (s1 * s1) * dPPDT));
+}
+
+// SRI fall-off function (fallOffFunctions.cpp:54-61, parameters a, b, c, d, e):
+//   F = d [a e^{-b/T} + e^{-T/c}]^X T^e,  X = 1 / (1 + log10(max(Pr, tiny))^2)
+__device__ __forceinline__ double sri_base(const double *s, double T) {
+    return s[0] * exp(-s[1] / T) + exp(-T / s[2]);
+}
+
+__device__ __forceinline__ double sri_F(const double *s, double T, double Pr) {
+    const double logPr = log10(hmax(Pr, kTiny));
+    const double X = 1.0 / (1.0 + logPr * logPr);
+    return s[3] * pow(sri_base(s, T), X) * pow(T, s[4]);
+}
+
+// The factor f of SRI::DFDci (fallOffFunctions.cpp:63-69) written as
+// DFDci = f * (1/Pr * dPr/dci):
+// f = F * (-2 X^2 log10(Pr) / ln 10) * ln(a e^{-b/T} + e^{-T/c})
+__device__ __forceinline__ double sri_dfdci_factor(const double *s, double T, double Pr,
+                                                   double F) {
+    const double lp = log10(hmax(Pr, kTiny));
+    const double X = 1.0 / (1.0 + lp * lp);
+    return F * (-X * X * 2.0 * log10(Pr) / log(10.0)) * log(sri_base(s, T));
+}
+
+// SRI::DFDT (fallOffFunctions.cpp:71-79)
+__device__ __forceinline__ double sri_dfdt(const double *s, double T, double Pr, double F,
+                                           double DPrDT) {
+    const double lp = log10(hmax(Pr, kTiny));
+    const double X = 1.0 / (1.0 + lp * lp);
+    const double dXdPr = -X * X * 2.0 * log10(Pr) / Pr / log(10.0);
+    const double eb = exp(-s[1] / T), ec = exp(-T / s[2]);
+    const double base = s[0] * eb + ec;
+    return F * (s[4] / T + dXdPr * DPrDT * log(base) +
+                X * (s[0] * s[1] * eb / (T * T) - ec / s[2]) / base);
 }
 
 struct IntegratorParams {

@@ -24,9 +24,19 @@ order, as the reference so that the tables hold identical bits:
 * third-body efficiencies default to 1.0 for every species
   (chemkinFileRead.cpp:1050-1061, :1063-1085).
 
+* units: the REACTIONS line may name the units of A (MOLES, MOLECULES) and
+  of E (CAL/MOLE, KCAL/MOLE, JOULES/MOLE, KJOULES/MOLE, KELVINS, EVOLTS),
+  and a reaction may override them with UNITS /.../; the factors are those
+  of chemkinFileRead::changeUnit (chemkinFileRead.cpp:1654-1696), with the
+  order of a side taken from its reaction orders (after FORD / RORD).
+
 Supported rate forms: Arrhenius, Arrhenius third-body (+M), unimolecular
-fall-off (+M) with Lindemann or Troe (3 or 4 parameters); reversible (=, <=>)
-and irreversible (=>) reactions.
+fall-off (+M) with Lindemann, Troe (3 or 4 parameters) or SRI (3 or 5
+parameters); reversible (=, <=>) and irreversible (=>) reactions; explicit
+reverse Arrhenius parameters (REV, reversibleReactionWithRevPars) on
+Arrhenius and third-body reactions; non-stoichiometric orders (FORD, RORD).
+The reference's other rate forms (PLOG, CHEB, HIGH, LT, JAN, ...) are
+rejected with NotImplementedError.
 """
 from __future__ import annotations
 
@@ -61,6 +71,23 @@ RATE_THIRD_BODY = 1
 RATE_LINDEMANN = 2
 RATE_TROE3 = 3
 RATE_TROE4 = 4
+RATE_SRI = 5
+
+# reversibility codes
+IRREVERSIBLE = 0
+REVERSIBLE = 1
+REVERSIBLE_REV = 2     # explicit reverse Arrhenius parameters
+
+# Chemkin unit keywords (chemkinFileRead.cpp:45-73)
+UNITS_A = {"MOLE": "MOLES", "MOLES": "MOLES", "MOLEC": "MOLECULES", "MOLECULE": "MOLECULES",
+           "MOLECULES": "MOLECULES"}
+UNITS_E = {"CAL": "CAL", "CAL/MOLE": "CAL", "EVOL": "EVOL", "EVOLTS": "EVOL", "JOUL": "JOUL",
+           "JOULES/MOLE": "JOUL", "KCAL": "KCAL", "KCAL/MOLE": "KCAL", "KELV": "KELV",
+           "KELVINS": "KELV", "KJOU": "KJOU", "KJOULES/MOLE": "KJOU"}
+ELECTRON_VOLT = 1.6021766208e-19    # J (physicalConstant.hpp:59,114)
+# auxiliary keywords of the reference's reader that this reader does not take
+_UNSUPPORTED_AUX = {"PLOG", "CHEB", "PCHEB", "TCHEB", "HIGH", "LT", "RLT", "JAN", "FIT1", "TDEP",
+                    "XSMI", "MOME", "EXCI", "COLLEFF"}
 
 
 @dataclasses.dataclass
@@ -75,6 +102,12 @@ class ParsedReaction:
     eff: Optional[np.ndarray] = None
     low: Optional[Tuple[float, float, float]] = None
     troe: Optional[List[float]] = None
+    sri: Optional[List[float]] = None
+    rev: Optional[Tuple[float, float, float]] = None
+    ford: Optional[Dict[int, float]] = None     # species -> forward order (FORD)
+    rord: Optional[Dict[int, float]] = None     # species -> reverse order (RORD)
+    units_A: str = "MOLES"
+    units_E: str = "CAL"
 
 
 @dataclasses.dataclass
@@ -109,6 +142,8 @@ class MechTables:
     dipole: np.ndarray
     polar: np.ndarray
     zrot: np.ndarray
+    sri: Optional[np.ndarray] = None       # [nrc, 5] a, b, c, d, e (SRI fall-off)
+    arr_rev: Optional[np.ndarray] = None   # [nrc, 3] explicit reverse A, beta, Ta (REV)
 
     @property
     def nsp(self) -> int:
@@ -156,6 +191,34 @@ def _split_side_terms(side: str) -> str:
     return side
 
 
+def _unit(word: str, where: str) -> Tuple[str, str]:
+    w = word.strip().upper()
+    if w in UNITS_A:
+        return "A", UNITS_A[w]
+    if w in UNITS_E:
+        return "E", UNITS_E[w]
+    raise ValueError(f"unknown unit {word!r} {where}")
+
+
+def change_unit(order: float, units_A: str, units_E: str, third_body: bool) -> Tuple[float, float]:
+    """(A factor, E factor) of chemkinFileRead::changeUnit (chemkinFileRead.cpp:1654-1696):
+    A [units_A, cm, s] -> [kmol, m^3, s] for a side of total order `order`,
+    and the divisor that turns E [units_E] into an activation temperature."""
+    RRjoule = R_J_MOL_K
+    RRcal = RRjoule / CAL_TH
+    if units_A == "MOLECULES":
+        Af = math.pow(NA, order) if third_body else math.pow(NA, order - 1.0)
+        Af *= math.pow(0.001, order - 1.0)
+    else:
+        Af = math.pow(0.001, order - 1.0)
+    Ef = {"CAL": RRcal, "KCAL": RRcal / 1000.0, "EVOL": RRjoule / ELECTRON_VOLT,
+          "JOUL": RRjoule, "KJOU": RRjoule / 1000.0, "KELV": 1.0}[units_E]
+    return Af, Ef
+
+
+_AUX_RE = re.compile(r"(\S+?)\s*/\s*([^/]*?)\s*/|(\S+)")
+
+
 def parse_chemkin(che_text: str, species_names: Optional[List[str]] = None):
     text = _strip_comments(che_text)
     sp_txt = _section(text, r"SPEC(?:|IE|IES)")
@@ -163,7 +226,15 @@ def parse_chemkin(che_text: str, species_names: Optional[List[str]] = None):
     index = {n: i for i, n in enumerate(names)}
     el_txt = _section(text, r"ELEM(?:|ENT|ENTS)")
     elements = [e.upper() for e in el_txt.split()]
-    rx_txt = _section(text, r"REAC(?:|TION|TIONS)")
+    # REACTIONS [units of A] [units of E] on its own line, then the reactions
+    # up to END (chemkinFileRead.cpp:1197-1284 for the units)
+    m = re.search(r"\bREAC(?:TIONS|TION|)\b([^\n]*)\n([\s\S]*?)(?:^|\n)[ \t]*END\b", text,
+                  re.IGNORECASE | re.MULTILINE)
+    header, rx_txt = (m.group(1), m.group(2)) if m else ("", "")
+    units = {"A": "MOLES", "E": "CAL"}
+    for word in header.split():
+        kind, u = _unit(word, "on the REACTIONS line")
+        units[kind] = u
     lines = [l for l in rx_txt.splitlines() if l.strip()]
     line_re = re.compile(r"^(.*?)\s*(<=>|=>|=)\s*(.*?)\s+([-+]?[0-9.]+(?:[eEdD][-+]?[0-9]+)?)"
                          r"\s+(\S+)\s+(\S+)\s*$")
@@ -171,7 +242,7 @@ def parse_chemkin(che_text: str, species_names: Optional[List[str]] = None):
     cur: Optional[ParsedReaction] = None
     for line in lines:
         m = line_re.match(line.strip())
-        if m and ("=" in m.group(2)):
+        if m and ("=" in m.group(2)) and "/" not in m.group(1):
             lhs, arrow, rhs = m.group(1), m.group(2), m.group(3)
             A, b, E = _read_real(m.group(4)), _read_real(m.group(5)), _read_real(m.group(6))
             kind = "arrhenius"
@@ -187,27 +258,60 @@ def parse_chemkin(che_text: str, species_names: Optional[List[str]] = None):
                 lhs, rhs = tb.sub("", lhs), tb.sub("", rhs)
                 kind = "third_body"
             cur = ParsedReaction(_parse_side(lhs, index), _parse_side(rhs, index),
-                                 arrow != "=>", A, b, E, kind)
+                                 arrow != "=>", A, b, E, kind,
+                                 units_A=units["A"], units_E=units["E"])
             if kind in ("third_body", "falloff"):
                 cur.eff = np.ones(len(names))
             reactions.append(cur)
             continue
-        # auxiliary line
-        s = line.strip()
-        up = s.upper()
-        if up.startswith("LOW"):
-            v = re.search(r"LOW\s*/\s*(.*?)\s*/", s, re.IGNORECASE).group(1).split()
-            cur.low = (_read_real(v[0]), _read_real(v[1]), _read_real(v[2]))
-        elif up.startswith("TROE"):
-            v = re.search(r"TROE\s*/\s*(.*?)\s*/", s, re.IGNORECASE).group(1).split()
-            cur.troe = [_read_real(x) for x in v]
-        elif up.startswith("DUP"):
-            continue
-        else:
-            for nm, val in re.findall(r"(\S+?)\s*/\s*([^/]+?)\s*/", s):
-                if nm not in index:
-                    raise ValueError(f"unknown efficiency species {nm!r}")
-                cur.eff[index[nm]] = _read_real(val)
+        # auxiliary line: KEY / values / groups, bare words, species efficiencies
+        if cur is None:
+            raise ValueError(f"auxiliary data before the first reaction: {line.strip()!r}")
+        for key, val, word in _AUX_RE.findall(line.strip()):
+            if word:
+                if word.upper() in ("DUP", "DUPLICATE"):
+                    continue
+                raise ValueError(f"unexpected word {word!r} in {line.strip()!r}")
+            up = key.upper()
+            v = val.split()
+            if up in _UNSUPPORTED_AUX:
+                raise NotImplementedError(f"rate form {up} is not supported by this reader")
+            if up == "LOW":
+                cur.low = (_read_real(v[0]), _read_real(v[1]), _read_real(v[2]))
+            elif up == "TROE":
+                cur.troe = [_read_real(x) for x in v]
+            elif up == "SRI":
+                if len(v) not in (3, 5):
+                    raise ValueError("SRI takes 3 or 5 parameters")
+                cur.sri = [_read_real(x) for x in v]
+            elif up == "REV":
+                cur.rev = (_read_real(v[0]), _read_real(v[1]), _read_real(v[2]))
+            elif up in ("FORD", "RORD"):
+                name, order = v[0], _read_real(v[1])
+                side = cur.fwd if up == "FORD" else cur.bwd
+                if name not in index or index[name] not in [i for i, _ in side]:
+                    # chemkinFileRead.cpp:974-1000
+                    raise ValueError(f"{up} species {name!r} is not on that side of the reaction")
+                d = cur.ford if up == "FORD" else cur.rord
+                if d is None:
+                    d = {}
+                    if up == "FORD":
+                        cur.ford = d
+                    else:
+                        cur.rord = d
+                d[index[name]] = order
+            elif up == "UNITS":
+                kind_u, u = _unit(val, "in UNITS")
+                if kind_u == "A":
+                    cur.units_A = u
+                else:
+                    cur.units_E = u
+            else:
+                if key not in index:
+                    raise ValueError(f"unknown efficiency species {key!r}")
+                if cur.eff is None:
+                    raise ValueError(f"efficiencies on a reaction without a third body: {line!r}")
+                cur.eff[index[key]] = _read_real(val)
     return names, elements, reactions
 
 
@@ -304,6 +408,8 @@ def compile_mechanism(che_path: str, thermo_path: str, transport_path: str) -> M
     arr = np.zeros((nrc, 3))
     arr0 = np.zeros((nrc, 3))
     troe = np.zeros((nrc, 4))
+    sri = np.zeros((nrc, 5))
+    arr_rev = np.zeros((nrc, 3))
     eff = np.ones((nrc, nsp))
     nf = np.zeros(nrc, np.int32)
     nb = np.zeros(nrc, np.int32)
@@ -314,15 +420,18 @@ def compile_mechanism(che_path: str, thermo_path: str, transport_path: str) -> M
     ford = np.zeros((nrc, MAX_SIDE))
     bord = np.zeros((nrc, MAX_SIDE))
     sum_stoi = np.zeros(nrc)
-    RRcal = R_J_MOL_K / CAL_TH
     for r, rx in enumerate(reactions):
         if len(rx.fwd) > MAX_SIDE or len(rx.bwd) > MAX_SIDE:
             raise ValueError("too many species on one side")
+        fo = [(rx.ford or {}).get(i, nu) for i, nu in rx.fwd]
+        bo = [(rx.rord or {}).get(i, nu) for i, nu in rx.bwd]
+        # the A factor follows the side's total reaction order, summed in
+        # the side's (name-sorted) order (chemkinFileRead.cpp:1365-1371)
         order = 0.0
-        for (_, nu) in rx.fwd:
-            order += nu
-        Afac = math.pow(0.001, order - 1.0)
-        Efac = RRcal
+        for o in fo:
+            order += o
+        third = rx.kind != "arrhenius"
+        Afac, Efac = change_unit(order, rx.units_A, rx.units_E, third)
         if rx.kind == "arrhenius":
             rate_type[r] = RATE_ARRHENIUS
             arr[r] = (rx.A * Afac, rx.b, rx.E / Efac)
@@ -333,11 +442,16 @@ def compile_mechanism(che_path: str, thermo_path: str, transport_path: str) -> M
         else:
             if rx.low is None:
                 raise ValueError("fall-off reaction without LOW")
+            if rx.rev is not None:
+                raise ValueError("REV cannot be used with a fall-off rate (chemkinFileRead.cpp:1460)")
             A0, b0, E0 = rx.low
             arr0[r] = (A0 * (1e-3 * Afac), b0, E0 / Efac)
             arr[r] = (rx.A * Afac, rx.b, rx.E / Efac)
             eff[r] = rx.eff
-            if rx.troe is None:
+            if rx.sri is not None:
+                rate_type[r] = RATE_SRI
+                sri[r] = rx.sri if len(rx.sri) == 5 else list(rx.sri) + [1.0, 0.0]
+            elif rx.troe is None:
                 rate_type[r] = RATE_LINDEMANN
             elif len(rx.troe) == 3:
                 rate_type[r] = RATE_TROE3
@@ -345,14 +459,26 @@ def compile_mechanism(che_path: str, thermo_path: str, transport_path: str) -> M
             else:
                 rate_type[r] = RATE_TROE4
                 troe[r, :4] = rx.troe[:4]
-        rev[r] = 1 if rx.reversible else 0
+        if rx.rev is not None:
+            # reversibleReactionWithRevPars: the reverse Arrhenius (or third-body)
+            # law with its own A factor from the reverse side's order
+            # (chemkinFileRead.cpp:1378-1380, 1387-1421)
+            border = 0.0
+            for o in bo:
+                border += o
+            AfR, EfR = change_unit(border, rx.units_A, rx.units_E, third)
+            Ar, br, Er = rx.rev
+            arr_rev[r] = ((1e-3 * Ar * AfR) if third else (Ar * AfR), br, Er / EfR)
+            rev[r] = REVERSIBLE_REV
+        else:
+            rev[r] = REVERSIBLE if rx.reversible else IRREVERSIBLE
         nf[r], nb[r] = len(rx.fwd), len(rx.bwd)
         s = 0.0
         for k, (i, nu) in enumerate(rx.fwd):
-            fidx[r, k], fnu[r, k], ford[r, k] = i, nu, nu
+            fidx[r, k], fnu[r, k], ford[r, k] = i, nu, fo[k]
             s -= nu
         for k, (i, nu) in enumerate(rx.bwd):
-            bidx[r, k], bnu[r, k], bord[r, k] = i, nu, nu
+            bidx[r, k], bnu[r, k], bord[r, k] = i, nu, bo[k]
             s += nu
         sum_stoi[r] = s
 
@@ -368,7 +494,7 @@ def compile_mechanism(che_path: str, thermo_path: str, transport_path: str) -> M
             geom[i], eps[i], sig[i], dip[i], pol[i], zr[i] = g, e_, s_, d_, p_, z_
     return MechTables(names, W, Ri, Tr, nasa, el_names, E, rate_type, rev, arr, arr0, troe,
                       eff, nf, nb, fidx, bidx, fnu, bnu, ford, bord, sum_stoi,
-                      geom, eps, sig, dip, pol, zr)
+                      geom, eps, sig, dip, pol, zr, sri=sri, arr_rev=arr_rev)
 
 
 def element_matrix_mass(m: MechTables) -> np.ndarray:

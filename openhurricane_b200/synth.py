@@ -63,6 +63,11 @@ class Reaction:
     eff: Dict[str, float] = dataclasses.field(default_factory=dict)
     low: Optional[Tuple[float, float, float]] = None
     troe: Optional[Tuple[float, ...]] = None
+    sri: Optional[Tuple[float, ...]] = None            # SRI a, b, c[, d, e] (replaces TROE)
+    rev: Optional[Tuple[float, float, float]] = None   # REV A, b, Ea (cm-mol-s, cal/mol)
+    ford: Dict[str, float] = dataclasses.field(default_factory=dict)
+    rord: Dict[str, float] = dataclasses.field(default_factory=dict)
+    units: Optional[str] = None                        # UNITS /.../ of this reaction
 
 
 @dataclasses.dataclass
@@ -70,6 +75,7 @@ class Mechanism:
     species: List[Species]
     reactions: List[Reaction]
     seed: int
+    units: Tuple[str, ...] = ()    # unit words on the REACTIONS line
 
     @property
     def names(self) -> List[str]:
@@ -307,6 +313,49 @@ def make_mechanism(nsp: int, nrc: int, n_third_body: int, n_troe: int,
     return Mechanism(species, reactions, seed)
 
 
+def extended_mechanism(seed: int = 20241117) -> Mechanism:
+    """9 species / 21 reactions using every rate form the reader takes beyond
+    the small mechanism's: two SRI fall-off reactions (3 and 5 parameters) and
+    one Troe, explicit reverse parameters (REV) on two Arrhenius and one
+    third-body reaction, a forward and a reverse order override (FORD 1.5,
+    RORD 1.5), energies written in kJ/mol on the REACTIONS line, and
+    per-reaction UNITS (molecules for one reaction, kcal/mol for another).
+    The rate parameters stay those of the drawn mechanism; the file carries
+    them in the declared units. (Orders below one give rates that are not
+    Lipschitz at zero concentration; with such an order this mechanism's
+    cells answer one-ulp input changes with 1e-6 changes of T, which no
+    parity tolerance between two libms survives, so both overrides are 1.5.)"""
+    m = make_mechanism(9, 21, 3, 3, seed)
+    rng = np.random.default_rng(seed + 1)
+    m.units = ("KJOU", "MOLES")
+    fall = [r for r in m.reactions if r.kind == "troe"]
+    fall[0].sri = (float(np.round(rng.uniform(0.5, 2.0), 4)),
+                   float(np.round(rng.uniform(100.0, 800.0), 1)),
+                   float(np.round(rng.uniform(500.0, 2000.0), 1)))
+    fall[0].troe = None
+    fall[1].sri = (float(np.round(rng.uniform(0.5, 2.0), 4)),
+                   float(np.round(rng.uniform(100.0, 800.0), 1)),
+                   float(np.round(rng.uniform(500.0, 2000.0), 1)),
+                   float(np.round(rng.uniform(0.8, 1.2), 4)),
+                   float(np.round(rng.uniform(-0.3, 0.3), 4)))
+    fall[1].troe = None
+    plain = [r for r in m.reactions if r.kind == "plain"]
+    tb = [r for r in m.reactions if r.kind == "third_body"]
+
+    def draw_rev():
+        return (10.0 ** rng.uniform(9.0, 13.0), float(np.round(rng.uniform(-0.8, 0.8), 4)),
+                float(np.round(rng.uniform(0.0, 40.0), 3)) * 1000.0)
+
+    plain[0].rev = draw_rev()
+    plain[1].rev = draw_rev()
+    tb[0].rev = draw_rev()
+    plain[2].ford = {plain[2].reactants[0][0]: 1.5}
+    plain[3].rord = {plain[3].products[0][0]: 1.5}
+    plain[4].units = "MOLEC"
+    plain[5].units = "KCAL"
+    return m
+
+
 def small_mechanism(seed: int = 20240901) -> Mechanism:
     """9 species / 21 reversible Arrhenius reactions, 3 third-body, 1 Troe."""
     return make_mechanism(9, 21, 3, 1, seed)
@@ -336,6 +385,30 @@ def _reaction_side(side: Sequence[Tuple[str, int]], kind: str) -> str:
     return txt
 
 
+def _energy_in(ea_cal: float, unit: str) -> float:
+    """An activation energy given in cal/mol, expressed in `unit`."""
+    if unit in ("CAL", "CAL/MOLE"):
+        return ea_cal
+    if unit in ("KCAL", "KCAL/MOLE"):
+        return ea_cal / 1000.0
+    if unit in ("JOUL", "JOULES/MOLE"):
+        return ea_cal * 4.184
+    if unit in ("KJOU", "KJOULES/MOLE"):
+        return ea_cal * 4.184 / 1000.0
+    if unit in ("KELV", "KELVINS"):
+        return ea_cal / (1.380649e-23 * 6.02214076e23 / 4.184)
+    raise ValueError(unit)
+
+
+def _pre_exp_in(a_mol: float, order: float, third: bool, unit: str) -> float:
+    """A pre-exponential factor in mol-cm-s units, expressed per molecule when
+    `unit` says MOLEC (the reader multiplies by NA^(order - 1), or NA^order
+    for a reaction with a third body)."""
+    if not unit.startswith("MOLEC"):
+        return a_mol
+    return a_mol / 6.02214076e23 ** (order if third else order - 1.0)
+
+
 def write_chemkin(mech: Mechanism, out_dir: str, stem: str = "mech") -> Tuple[str, str, str]:
     os.makedirs(out_dir, exist_ok=True)
     che = os.path.join(out_dir, f"{stem}.che")
@@ -347,16 +420,37 @@ def write_chemkin(mech: Mechanism, out_dir: str, stem: str = "mech") -> Tuple[st
     names = mech.names
     for i in range(0, len(names), 8):
         lines.append(" ".join(names[i:i + 8]))
-    lines += ["END", "REACTIONS"]
+    lines += ["END", "REACTIONS" + "".join(" " + u for u in mech.units)]
+    g_A = next((u for u in mech.units if u.startswith("MOLEC")), "MOLES")
+    g_E = next((u for u in mech.units if not u.startswith("MOLE")), "CAL")
     for r in mech.reactions:
+        u_A = r.units if (r.units or "").startswith("MOLEC") else g_A
+        u_E = r.units if (r.units and not r.units.startswith("MOLE")) else g_E
+        E = lambda ea: _energy_in(ea, u_E)
+        fo = sum(r.ford.get(s_, n) for s_, n in r.reactants)
+        bo = sum(r.rord.get(s_, n) for s_, n in r.products)
+        third = r.kind != "plain"
+        A = lambda a, o: _pre_exp_in(a, o, third, u_A)
         eq = _reaction_side(r.reactants, r.kind) + "=" + _reaction_side(r.products, r.kind)
-        lines.append(f"{eq}   {r.A:.6E}  {r.b:.6f}  {r.Ea:.4f}")
+        lines.append(f"{eq}   {A(r.A, fo):.6E}  {r.b:.6f}  {E(r.Ea):.4f}")
         if r.kind == "troe":
             A0, b0, E0 = r.low
-            lines.append(f"   LOW / {A0:.6E}  {b0:.6f}  {E0:.4f} /")
-            lines.append("   TROE / " + "  ".join(f"{x:.6g}" for x in r.troe) + " /")
+            lines.append(f"   LOW / {A(A0, fo):.6E}  {b0:.6f}  {E(E0):.4f} /")
+            if r.sri is not None:
+                lines.append("   SRI / " + "  ".join(f"{x:.6g}" for x in r.sri) + " /")
+            else:
+                lines.append("   TROE / " + "  ".join(f"{x:.6g}" for x in r.troe) + " /")
         if r.kind in ("third_body", "troe") and r.eff:
             lines.append("   " + " ".join(f"{k}/{v:.2f}/" for k, v in r.eff.items()))
+        if r.rev is not None:
+            Ar, br, Er = r.rev
+            lines.append(f"   REV / {A(Ar, bo):.6E}  {br:.6f}  {E(Er):.4f} /")
+        for k, v in r.ford.items():
+            lines.append(f"   FORD / {k} {v:g} /")
+        for k, v in r.rord.items():
+            lines.append(f"   RORD / {k} {v:g} /")
+        if r.units:
+            lines.append(f"   UNITS / {r.units} /")
     lines += ["END", ""]
     with open(che, "w") as f:
         f.write("\n".join(lines))

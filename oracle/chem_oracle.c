@@ -12,7 +12,8 @@
  *                 thermo/include/thermo.inl:44-203 (molar = mass x W)
  *   rate laws     reactionRateTypes/src/ArrheniusRR.cpp:37-47 (+ hpp:96-99),
  *                 ArrheniusThirdBodyRR.cpp:37-57, unimolecularFallOffRR.cpp:37-91,
- *                 fallOffFunctions.cpp:81-157 (Troe), fallOffFunctions.hpp (Lindemann)
+ *                 fallOffFunctions.cpp:81-157 (Troe), :54-79 (SRI), fallOffFunctions.hpp
+ *                 (Lindemann); reversibleReactionWithRevPars.hpp:68-122 (Chemkin REV)
  *   reactions     reactionTypes/src/reactionTypes.cpp:178-352 (Kp, DKpDT, Kc, DKcDT, q),
  *                 :354-445 (DqDci), :843-876 (DqDT); reversibleReactions.hpp:62-127;
  *                 irreversibleReactions.hpp; reactionList.hpp:83-86 (updateG0)
@@ -166,9 +167,33 @@ static void troeLogFcent(const double *tr, int four, double T, double *logFcent)
                                    exp(-Tss / T), TINY));
 }
 
+/* SRI (fallOffFunctions.cpp:54-79): a, b, c, d, e */
+static double sriF(const double *s, double T, double Pr) {
+    const double logPr = log10(hmax(Pr, TINY));
+    const double X = 1.0 / (1.0 + logPr * logPr);
+    return s[3] * pow(s[0] * exp(-s[1] / T) + exp(-T / s[2]), X) * pow(T, s[4]);
+}
+
+static double sriDFDci(const double *s, double T, double Pr, double F, double DPrDci) {
+    const double lp = log10(hmax(Pr, TINY));
+    const double X = 1.0 / (1.0 + lp * lp);
+    const double dXdc = -X * X * 2.0 * log10(Pr) / Pr / log(10.0) * DPrDci;
+    return (F * dXdc * log(s[0] * exp(-s[1] / T) + exp(-T / s[2])));
+}
+
+static double sriDFDT(const double *s, double T, double Pr, double F, double DPrDT) {
+    const double lp = log10(hmax(Pr, TINY));
+    const double X = 1.0 / (1.0 + lp * lp);
+    const double dXdPr = -X * X * 2.0 * log10(Pr) / Pr / log(10.0);
+    return (F * (s[4] / T + dXdPr * DPrDT * log(s[0] * exp(-s[1] / T) + exp(-T / s[2])) +
+                 X * (s[0] * s[1] * exp(-s[1] / T) / (T * T) - exp(-T / s[2]) / s[2]) /
+                     (s[0] * exp(-s[1] / T) + exp(-T / s[2]))));
+}
+
 static double fallF(const hc_mech_desc *m, int r, double T, double Pr) {
     const int t = m->rate_type[r];
     if (t == HC_RATE_LINDEMANN) return 1.0;
+    if (t == HC_RATE_SRI) return sriF(&m->sri[5 * r], T, Pr);
     double logFcent;
     troeLogFcent(&m->troe[4 * r], t == HC_RATE_TROE4, T, &logFcent);
     const double c = -0.4 - 0.67 * logFcent;
@@ -183,6 +208,7 @@ static double fallDFDci(const hc_mech_desc *m, int r, double T, double Pr, doubl
                         double DPrDci) {
     const int t = m->rate_type[r];
     if (t == HC_RATE_LINDEMANN) return 0.0;
+    if (t == HC_RATE_SRI) return sriDFDci(&m->sri[5 * r], T, Pr, F, DPrDci);
     const double logPr = log10(hmax(Pr, TINY));
     double logFcent;
     troeLogFcent(&m->troe[4 * r], t == HC_RATE_TROE4, T, &logFcent);
@@ -202,6 +228,7 @@ static double fallDFDT(const hc_mech_desc *m, int r, double T, double Pr, double
                        double DPrDT) {
     const int t = m->rate_type[r];
     if (t == HC_RATE_LINDEMANN) return 0.0;
+    if (t == HC_RATE_SRI) return sriDFDT(&m->sri[5 * r], T, Pr, F, DPrDT);
     const double *tr = &m->troe[4 * r];
     const double alpha = tr[0], Tsss = tr[1], Ts = tr[2], Tss = tr[3];
     const double ln10 = log(10.0);
@@ -354,7 +381,19 @@ static double DKcDT(const mech_ctx *x, int r, double T) {
     return v;
 }
 
-static double kRev(const mech_ctx *x, int r, double kfwd, double T) {
+/* explicit reverse rate (reversibleReactionWithRevPars::kr): the reverse
+   Arrhenius law, or the third-body one, M times it */
+static double kRevExplicit(const hc_mech_desc *m, int r, double T, const double *c) {
+    const double *a = &m->arr_rev[3 * r];
+    if (m->rate_type[r] == HC_RATE_THIRD_BODY) {
+        const double M = thirdM(m, r, c);
+        return (M * arrK(a, T));
+    }
+    return arrK(a, T);
+}
+
+static double kRev(const mech_ctx *x, int r, double kfwd, double T, const double *c) {
+    if (x->m->reversible[r] == HC_REVERSIBLE_REV) return kRevExplicit(x->m, r, T, c);
     if (!x->m->reversible[r]) return 0.0;
     const double kc = Kc(x, r, T);
     if (fabs(kc) > VERY_TINY) return kfwd / kc;
@@ -362,6 +401,7 @@ static double kRev(const mech_ctx *x, int r, double kfwd, double T) {
 }
 
 static double DkrDT(const mech_ctx *x, int r, double kr, double T, double dkfdT) {
+    if (x->m->reversible[r] == HC_REVERSIBLE_REV) return arrDkDT(&x->m->arr_rev[3 * r], kr, T);
     if (!x->m->reversible[r]) return 0.0;
     const double kc = hmax(Kc(x, r, T), VERY_TINY);
     return (dkfdT - kr * DKcDT(x, r, T)) / kc;
@@ -373,7 +413,7 @@ static double qRate(const mech_ctx *x, int r, double T, const double *c, double 
     const hc_mech_desc *m = x->m;
     double qf = rateK(m, r, T, c);
     if (kfo) *kfo = qf;
-    double qr = kRev(x, r, qf, T);
+    double qr = kRev(x, r, qf, T, c);
     if (kro) *kro = qr;
     for (int k = 0; k < m->nf[r]; ++k)
         qf *= pow(hmax(c[m->fidx[HC_MAX_SIDE * r + k]], 0.0), m->ford[HC_MAX_SIDE * r + k]);
@@ -817,7 +857,7 @@ void oracle_rates(const hc_mech_desc *m, double T, const double *c, double *out)
         const double kf = rateK(m, r, T, cc);
         out[3 * r] = kf;
         out[3 * r + 1] = Kc(&x, r, T);
-        out[3 * r + 2] = kRev(&x, r, kf, T);
+        out[3 * r + 2] = kRev(&x, r, kf, T, cc);
     }
     free(x.G0); free(x.DG0DT); free(cc);
 }

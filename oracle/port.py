@@ -26,6 +26,18 @@ def build(force: bool = False) -> str:
     return LIB
 
 
+def _sri(t):
+    """SRI parameters [nrc, 5] (zeros for tables without them)."""
+    a = getattr(t, "sri", None)
+    return np.zeros((t.nrc, 5)) if a is None else a
+
+
+def _arr_rev(t):
+    """Explicit reverse Arrhenius parameters [nrc, 3] (zeros for tables without them)."""
+    a = getattr(t, "arr_rev", None)
+    return np.zeros((t.nrc, 3)) if a is None else a
+
+
 class HcMechDesc(C.Structure):
     _fields_ = [
         ("nsp", C.c_int32), ("nrc", C.c_int32),
@@ -35,6 +47,7 @@ class HcMechDesc(C.Structure):
         ("nf", C.c_void_p), ("nb", C.c_void_p), ("fidx", C.c_void_p), ("bidx", C.c_void_p),
         ("fnu", C.c_void_p), ("bnu", C.c_void_p), ("ford", C.c_void_p), ("bord", C.c_void_p),
         ("geom", C.c_void_p), ("eps_k", C.c_void_p), ("sigma", C.c_void_p),
+        ("sri", C.c_void_p), ("arr_rev", C.c_void_p),
     ]
 
 
@@ -77,7 +90,7 @@ class MechDesc:
             arr0=f64(t.arr0), troe=f64(t.troe), eff=f64(t.eff), nf=i32(t.nf), nb=i32(t.nb),
             fidx=i32(t.fidx), bidx=i32(t.bidx), fnu=f64(t.fnu), bnu=f64(t.bnu),
             ford=f64(t.ford), bord=f64(t.bord), geom=i32(t.geom), eps_k=f64(t.eps_k),
-            sigma=f64(t.sigma))
+            sigma=f64(t.sigma), sri=f64(_sri(t)), arr_rev=f64(_arr_rev(t)))
         d = HcMechDesc()
         d.nsp, d.nrc = t.nsp, t.nrc
         for k, a in self.arrays.items():

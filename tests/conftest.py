@@ -20,7 +20,8 @@ def mech_dir(tmp_path_factory):
 
 def _make(name, mech_dir):
     from openhurricane_b200 import synth, mechanism
-    m = synth.small_mechanism() if name == "small" else synth.large_mechanism()
+    m = {"small": synth.small_mechanism, "large": synth.large_mechanism,
+         "ext": synth.extended_mechanism}[name]()
     d = os.path.join(mech_dir, name)
     che, th, tr = synth.write_chemkin(m, d)
     tables = mechanism.compile_mechanism(che, th, tr)
@@ -35,3 +36,9 @@ def small(mech_dir):
 @pytest.fixture(scope="session")
 def large(mech_dir):
     return _make("large", mech_dir)
+
+
+@pytest.fixture(scope="session")
+def ext(mech_dir):
+    """The small mechanism's species with SRI, REV, FORD / RORD and unit keywords."""
+    return _make("ext", mech_dir)

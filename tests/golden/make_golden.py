@@ -13,12 +13,18 @@ and stores inputs and outputs:
   large_ref.npz : 53-species / 325-reaction mechanism, 2 cells drawn like the
                   large workload (T 800-2800 K, p 0.5-10 atm, Dirichlet(0.3)),
                   dt = 1e-7 s; plus KAT states and properties of 16 cells.
+  ext_ref.npz   : 9-species / 21-reaction mechanism with the rate forms beyond
+                  the small one (SRI, REV, FORD / RORD, REACTIONS-line and
+                  per-reaction units; synth.extended_mechanism), 24 cells drawn
+                  like the small workload, dt = 1e-6 s; plus KAT states,
+                  point-implicit source terms and properties of 16 cells.
 
 The mechanism files are regenerated from their seeds by
 openhurricane_b200.synth at test time; a SHA-256 of the generated text files
 is stored so that a change of the generator is detected.
 
-    python tests/golden/make_golden.py   (needs oracle/_ref/hurchem_ref)
+    python tests/golden/make_golden.py [small] [large] [ext]   (default: all;
+    needs oracle/_ref/hurchem_ref)
 """
 import hashlib
 import os
@@ -94,15 +100,22 @@ def make(name, mech, cells, dt, nkat, prop_cells, out):
 def main():
     if not refrun.available():
         raise SystemExit("oracle/_ref/hurchem_ref is missing: make -f oracle/Makefile.ref")
-    small = synth.small_mechanism()
-    make("small", small, synth.dirichlet_cells(9, 48, seed=101), 1e-6, 8,
-         synth.dirichlet_cells(9, 32, seed=105), os.path.join(HERE, "small_ref.npz"))
-    large = synth.large_mechanism()
-    make("large", large, synth.dirichlet_cells(53, 2, seed=103, T_range=(800, 2800),
-                                               p_atm_range=(0.5, 10), alpha=0.3),
-         1e-7, 3, synth.dirichlet_cells(53, 16, seed=107, T_range=(800, 2800),
-                                         p_atm_range=(0.5, 10), alpha=0.3),
-         os.path.join(HERE, "large_ref.npz"))
+    which = set(sys.argv[1:]) or {"small", "large", "ext"}
+    if "small" in which:
+        small = synth.small_mechanism()
+        make("small", small, synth.dirichlet_cells(9, 48, seed=101), 1e-6, 8,
+             synth.dirichlet_cells(9, 32, seed=105), os.path.join(HERE, "small_ref.npz"))
+    if "large" in which:
+        large = synth.large_mechanism()
+        make("large", large, synth.dirichlet_cells(53, 2, seed=103, T_range=(800, 2800),
+                                                   p_atm_range=(0.5, 10), alpha=0.3),
+             1e-7, 3, synth.dirichlet_cells(53, 16, seed=107, T_range=(800, 2800),
+                                             p_atm_range=(0.5, 10), alpha=0.3),
+             os.path.join(HERE, "large_ref.npz"))
+    if "ext" in which:
+        ext = synth.extended_mechanism()
+        make("ext", ext, synth.dirichlet_cells(9, 24, seed=109), 1e-6, 8,
+             synth.dirichlet_cells(9, 16, seed=111), os.path.join(HERE, "ext_ref.npz"))
 
 
 if __name__ == "__main__":

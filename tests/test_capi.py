@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol():
     for name in declared_functions():
         assert hasattr(lib, name), name
         assert name in _capi.SIGNATURES, name
-    assert lib.hc_abi_version() == 1
+    assert lib.hc_abi_version() == 2
 
 
 def test_default_opts_match_reference_defaults():
@@ -53,3 +53,33 @@ def test_invalid_arguments_fail_loudly_without_gpu():
     assert lib.hc_mech_create(None, C.byref(h)) == -1
     assert b"null" in lib.hc_last_error()
     assert lib.hc_set_tuning(None, 0, 64) == -1
+
+
+def test_mechanism_checks_of_the_extended_rate_forms_without_gpu(ext):
+    """SRI and explicit reverse (REV) reactions: the generated thread-per-cell
+    kernel refuses them, and inconsistent tables are rejected before any
+    device work (hc_jit_source runs the mechanism checks on the host)."""
+    from openhurricane_b200 import _capi
+    lib = _capi.load()
+    n = C.c_int64()
+    a = _capi.DescArrays(ext["tables"])
+    assert lib.hc_jit_source(C.byref(a.desc), 64, None, 0, C.byref(n)) == -3
+    assert b"SRI" in lib.hc_last_error()
+
+    def bad(mutate, msg):
+        import copy
+        b = _capi.DescArrays(copy.deepcopy(ext["tables"]))    # the arrays may alias the tables
+        mutate(b)
+        assert lib.hc_jit_source(C.byref(b.desc), 64, None, 0, C.byref(n)) == -1
+        assert msg in lib.hc_last_error()
+
+    bad(lambda b: setattr(b.desc, "sri", None), b"SRI reaction without")
+    bad(lambda b: setattr(b.desc, "arr_rev", None), b"REV reaction without")
+
+    def rev_on_falloff(b):
+        b.arrays["reversible"][b.arrays["rate_type"] == 5] = 2
+    bad(rev_on_falloff, b"fall-off")
+
+    def bad_code(b):
+        b.arrays["reversible"][0] = 3
+    bad(bad_code, b"reversibility")

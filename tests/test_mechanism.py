@@ -60,3 +60,81 @@ def test_large_mechanism_shape_and_element_balance(large):
         for k in range(t.nb[r]):
             bal += t.bnu[r, k] * E[:, t.bidx[r, k]]
         assert np.all(bal == 0)
+
+
+def test_unit_factors_follow_the_reference_change_unit():
+    """chemkinFileRead::changeUnit: A from [mol or molecule, cm^3, s] to
+    [kmol, m^3, s], E to an activation temperature."""
+    R = M.R_J_MOL_K
+    for order in (1.0, 1.5, 2.0, 3.0):
+        Af, Ef = M.change_unit(order, "MOLES", "CAL", False)
+        assert Af == math.pow(0.001, order - 1.0) and Ef == R / M.CAL_TH
+        Af, _ = M.change_unit(order, "MOLECULES", "CAL", False)
+        assert Af == math.pow(M.NA, order - 1.0) * math.pow(0.001, order - 1.0)
+        Af, _ = M.change_unit(order, "MOLECULES", "CAL", True)
+        assert Af == math.pow(M.NA, order) * math.pow(0.001, order - 1.0)
+    E = {u: M.change_unit(2.0, "MOLES", u, False)[1]
+         for u in ("CAL", "KCAL", "JOUL", "KJOU", "KELV", "EVOL")}
+    assert E["KCAL"] == (R / M.CAL_TH) / 1000.0 and E["JOUL"] == R
+    assert E["KJOU"] == R / 1000.0 and E["KELV"] == 1.0 and E["EVOL"] == R / M.ELECTRON_VOLT
+
+
+def test_extended_rate_forms_are_read(ext):
+    t = ext["tables"]
+    m = ext["mech"]
+    assert m.units == ("KJOU", "MOLES")
+    sri = np.flatnonzero(t.rate_type == M.RATE_SRI)
+    assert len(sri) == 2
+    five = [r for r in m.reactions if r.sri is not None and len(r.sri) == 5][0]
+    three = [r for r in m.reactions if r.sri is not None and len(r.sri) == 3][0]
+    rows = {tuple(t.sri[r, :3]) for r in sri}
+    assert tuple(three.sri) in rows and tuple(five.sri[:3]) in rows
+    for r in sri:
+        if tuple(t.sri[r, :3]) == tuple(three.sri):
+            assert t.sri[r, 3] == 1.0 and t.sri[r, 4] == 0.0      # SRI(a, b, c): d = 1, e = 0
+        else:
+            assert tuple(t.sri[r]) == tuple(five.sri)
+    rev = np.flatnonzero(t.reversible == M.REVERSIBLE_REV)
+    assert len(rev) == 3
+    assert set(t.rate_type[rev]) == {M.RATE_ARRHENIUS, M.RATE_THIRD_BODY}
+    assert (t.arr_rev[rev, 0] > 0).all() and (t.arr_rev[t.reversible != 2] == 0).all()
+    # the FORD / RORD overrides change the order only, not the stoichiometry
+    assert (t.ford != t.fnu).sum() == 1 and t.ford[t.ford != t.fnu][0] == 1.5
+    assert (t.bord != t.bnu).sum() == 1 and t.bord[t.bord != t.bnu][0] == 1.5
+
+
+def test_energy_units_give_the_same_activation_temperature(tmp_path):
+    """The same reaction written with E in cal/mol, kcal/mol, kJ/mol and K
+    (REACTIONS-line and per-reaction units) reads to one activation
+    temperature, to the digits printed (four decimals of kcal/mol are 0.05 K)."""
+    from openhurricane_b200 import synth
+    base = synth.small_mechanism()
+    che, th, tr = synth.write_chemkin(base, str(tmp_path / "a"))
+    t0 = M.compile_mechanism(che, th, tr)
+    for units, per in ((("KCAL",), None), (("KJOU", "MOLES"), None), ((), "KELV")):
+        m = synth.small_mechanism()
+        m.units = units
+        if per:
+            for r in m.reactions:
+                r.units = per
+        che, th, tr = synth.write_chemkin(m, str(tmp_path / ("u" + "".join(units) + (per or ""))))
+        t = M.compile_mechanism(che, th, tr)
+        assert np.allclose(t.arr[:, 2], t0.arr[:, 2], rtol=0.0, atol=0.06)
+        assert np.array_equal(t.arr[:, 0], t0.arr[:, 0])
+
+
+def _che(body, header="REACTIONS"):
+    return ("ELEMENTS\nH O\nEND\nSPECIES\nH2 O2 H O HO\nEND\n" + header + "\n" + body + "\nEND\n")
+
+
+def test_reader_rejects_what_it_does_not_take():
+    import pytest
+    with pytest.raises(NotImplementedError, match="PLOG"):
+        M.parse_chemkin(_che("H2+O2=2HO 1.0E13 0.0 1000.0\n PLOG / 1.0 1.0E13 0.0 1000.0 /"))
+    with pytest.raises(ValueError, match="FORD"):
+        M.parse_chemkin(_che("H2+O2=2HO 1.0E13 0.0 1000.0\n FORD / O 0.5 /"))
+    with pytest.raises(ValueError, match="unit"):
+        M.parse_chemkin(_che("H2+O2=2HO 1.0E13 0.0 1000.0", header="REACTIONS FURLONGS"))
+    names, _, rx = M.parse_chemkin(_che(
+        "H+O2(+M)=HO+O(+M) 1.0E13 0.0 1000.0\n LOW / 1.0E16 0.0 0.0 /\n REV / 1.0E12 0.0 0.0 /"))
+    assert rx[0].rev is not None and rx[0].kind == "falloff"

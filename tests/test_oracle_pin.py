@@ -30,16 +30,16 @@ def _load(name):
     return np.load(os.path.join(HERE, "golden", f"{name}_ref.npz"))
 
 
-@pytest.mark.parametrize("name", ["small", "large"])
-def test_generator_reproduces_golden_mechanism(name, small, large):
-    mk = small if name == "small" else large
+@pytest.mark.parametrize("name", ["small", "large", "ext"])
+def test_generator_reproduces_golden_mechanism(name, request):
+    mk = request.getfixturevalue(name)
     assert _sha(mk["files"]) == str(_load(name)["sha"])
 
 
-@pytest.mark.parametrize("name", ["small", "large"])
-def test_oracle_integration_bit_exact_vs_reference_golden(name, small, large):
+@pytest.mark.parametrize("name", ["small", "large", "ext"])
+def test_oracle_integration_bit_exact_vs_reference_golden(name, request):
     from oracle import port
-    mk = small if name == "small" else large
+    mk = request.getfixturevalue(name)
     g = _load(name)
     md = port.MechDesc(mk["tables"])
     o = port.integrate(md, g["in_T"], g["in_p"], g["in_rho"], g["in_Y"], float(g["dt"]),
@@ -48,10 +48,10 @@ def test_oracle_integration_bit_exact_vs_reference_golden(name, small, large):
         assert np.array_equal(o[k], g["out_" + k]), k
 
 
-@pytest.mark.parametrize("name", ["small", "large"])
-def test_oracle_kernels_bit_exact_vs_reference_golden(name, small, large):
+@pytest.mark.parametrize("name", ["small", "large", "ext"])
+def test_oracle_kernels_bit_exact_vs_reference_golden(name, request):
     from oracle import port
-    mk = small if name == "small" else large
+    mk = request.getfixturevalue(name)
     g = _load(name)
     md = port.MechDesc(mk["tables"])
     dydt, J = port.rhs_jac(md, g["kat_c"], g["kat_T"])
@@ -62,10 +62,10 @@ def test_oracle_kernels_bit_exact_vs_reference_golden(name, small, large):
         assert np.array_equal(port.rates(md, g["kat_T"][s], g["kat_c"][:, s]), g["kat_rates"][s])
 
 
-@pytest.mark.parametrize("name", ["small", "large"])
-def test_property_oracle_vs_reference_golden(name, small, large):
+@pytest.mark.parametrize("name", ["small", "large", "ext"])
+def test_property_oracle_vs_reference_golden(name, request):
     from oracle import props_oracle
-    mk = small if name == "small" else large
+    mk = request.getfixturevalue(name)
     g = _load(name)
     o = props_oracle.properties(mk["tables"], g["prop_T"], g["prop_p"], g["prop_Y"])
     for k in ("ha", "cp", "mu", "kappa", "D"):
@@ -93,11 +93,11 @@ def test_oracle_bit_exact_vs_reference_binary(small):
     assert o["status"][0] == 1 and r["status"][0] == 1
 
 
-@pytest.mark.parametrize("name", ["small", "large"])
-def test_point_implicit_oracle_vs_reference_golden(name, small, large):
+@pytest.mark.parametrize("name", ["small", "large", "ext"])
+def test_point_implicit_oracle_vs_reference_golden(name, request):
     """Ri and the diagonal source Jacobian of calculateSourceTermsImp."""
     from oracle import srcimp_oracle
-    mk = small if name == "small" else large
+    mk = request.getfixturevalue(name)
     g = _load(name)
     o = srcimp_oracle.srcimp(mk["tables"], g["prop_T"], g["prop_p"], g["prop_rho"], g["prop_Y"])
     assert np.array_equal(o["Ri"], g["srcimp_Ri"])
@@ -106,12 +106,12 @@ def test_point_implicit_oracle_vs_reference_golden(name, small, large):
     assert (np.abs(o["diag"] - ref) / scale).max() < 1e-14
 
 
-@pytest.mark.parametrize("name", ["small", "large"])
-def test_temperature_from_enthalpy_oracle_vs_reference_golden(name, small, large):
+@pytest.mark.parametrize("name", ["small", "large", "ext"])
+def test_temperature_from_enthalpy_oracle_vs_reference_golden(name, request):
     """thermoList::THa_p: Newton on the mixture enthalpy with the reference's
     tolerance, iteration cap and [TLow, THigh] clamp."""
     from oracle import props_oracle
-    mk = small if name == "small" else large
+    mk = request.getfixturevalue(name)
     g = _load(name)
     T, flag = props_oracle.temperature_from_ha(mk["tables"], g["tha_ha"], g["prop_p"], g["prop_Y"],
                                                g["tha_T0"])

@@ -119,6 +119,56 @@ def test_small_mechanism_parity_vs_oracle(small, kernel, block):
     assert (np.abs(g["Ri"] - Ri_o) / scale).max() < 1e-5
 
 
+@pytest.mark.parametrize("kernel", [0, 2])
+def test_extended_rate_forms_parity_vs_oracle(ext, kernel):
+    """SRI fall-off, explicit reverse parameters (REV) on Arrhenius and
+    third-body reactions, FORD / RORD orders and unit keywords, through the
+    cell-group kernels, against the oracle (pinned to the reference on this
+    mechanism). These cells take at most 73945 Newton iterations each in the
+    oracle (a few seconds of cell-group time); the GPU run carries a cap of
+    1000000 per cell so that a cell taking another path ends the test with a
+    failure instead of running on."""
+    t = ext["tables"]
+    assert (t.rate_type == 5).sum() == 2 and (t.reversible == 2).sum() == 3
+    T, p, rho, Y = _cells(t, 128, seed=13)
+    m = _mech(t)
+    m.set_tuning(kernel, 64)
+    g = _gpu_integrate(m, T, p, rho, Y, 1e-6, max_newton_total=1000000, **PARITY)
+    o = _oracle(t, T, p, rho, Y, 1e-6, key="ext128", **PARITY)
+    assert np.array_equal(g["status"] & 12, np.zeros_like(g["status"]))
+    _assert_close(g, o, f"extended forms, kernel {kernel}")
+    c0 = rho[None, :] * Y / t.W[:, None]
+    Ri_o = (o["c"] - c0) / 1e-6 * t.W[:, None]
+    scale = np.abs(Ri_o).max(axis=0, keepdims=True) + 1e-300
+    assert (np.abs(g["Ri"] - Ri_o) / scale).max() < 1e-5
+
+
+@pytest.mark.parametrize("kernel", [1, 3, 4])
+def test_extended_rate_forms_refused_by_thread_per_cell_kernels(ext, kernel):
+    from openhurricane_b200 import _capi
+    t = ext["tables"]
+    T, p, rho, Y = _cells(t, 8, seed=14)
+    m = _mech(t)
+    m.set_tuning(kernel, 64)
+    with pytest.raises(_capi.HcError, match="SRI"):
+        _gpu_integrate(m, T, p, rho, Y, 1e-6, **PARITY)
+
+
+def test_extended_rate_forms_source_terms_vs_oracle(ext):
+    from oracle import port
+    dev = _cuda()
+    t = ext["tables"]
+    T, p, rho, Y = _cells(t, 256, seed=15)
+    m = _mech(t)
+    d = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+    Ri = m.source_terms(d(T), d(p), d(rho), d(Y)).cpu().numpy()
+    c = rho[None, :] * Y / t.W[:, None]
+    f, _ = port.rhs_jac(port.MechDesc(t), c, T)
+    ref = f[:, : t.nsp].T * t.W[:, None]
+    sc = np.abs(ref).max(axis=0, keepdims=True) + 1e-300
+    assert (np.abs(Ri - ref) / sc).max() < 1e-11
+
+
 @pytest.mark.parametrize("kernel,block", [(0, 64)])
 def test_large_mechanism_parity_vs_oracle(large, kernel, block):
     from openhurricane_b200 import workloads
@@ -133,15 +183,18 @@ def test_large_mechanism_parity_vs_oracle(large, kernel, block):
     _assert_close(g, o, "large")
 
 
-@pytest.mark.parametrize("name", ["small", "large"])
-def test_against_reference_golden_outputs(name, small, large):
+@pytest.mark.parametrize("name", ["small", "large", "ext"])
+def test_against_reference_golden_outputs(name, request):
     """The reference's own outputs (default rtol 1e-4, atol 1e-15): most cells
     agree to the parity tolerance and every cell agrees to the solver's rtol."""
-    mk = small if name == "small" else large
+    mk = request.getfixturevalue(name)
     g0 = _golden(name)
     m = _mech(mk["tables"])
+    # the extended mechanism's reference cells take up to 148592 Newton
+    # iterations each; a cap bounds a cell that would take another path
+    cap = dict(max_newton_total=1000000) if name == "ext" else {}
     g = _gpu_integrate(m, g0["in_T"], g0["in_p"], g0["in_rho"], g0["in_Y"], float(g0["dt"]),
-                       atol=1e-15)
+                       atol=1e-15, **cap)
     dT = np.abs(g["T"] - g0["out_T"]) / g0["out_T"]
     assert dT.max() < 1e-4
     dY = np.abs(g["Y"] - g0["out_Y"]) - Y_RTOL * np.abs(g0["out_Y"]) - Y_FLOOR
@@ -149,9 +202,9 @@ def test_against_reference_golden_outputs(name, small, large):
     assert ok.mean() >= 0.9, f"{ok.mean():.3f} of cells within parity tolerance"
 
 
-@pytest.mark.parametrize("name", ["small", "large"])
-def test_rhs_jacobian_vs_reference_golden(name, small, large):
-    mk = small if name == "small" else large
+@pytest.mark.parametrize("name", ["small", "large", "ext"])
+def test_rhs_jacobian_vs_reference_golden(name, request):
+    mk = request.getfixturevalue(name)
     g0 = _golden(name)
     dev = _cuda()
     m = _mech(mk["tables"])
@@ -307,12 +360,12 @@ def test_graph_captured_step_matches_eager(which, small, large):
     del g
 
 
-@pytest.mark.parametrize("name", ["small", "large"])
-def test_point_implicit_source_terms_vs_reference_golden(name, small, large):
+@pytest.mark.parametrize("name", ["small", "large", "ext"])
+def test_point_implicit_source_terms_vs_reference_golden(name, request):
     """hc_source_terms_imp against the reference's calculateSourceTermsImp
     outputs and the oracle on fresh cells."""
     from oracle import srcimp_oracle
-    mk = small if name == "small" else large
+    mk = request.getfixturevalue(name)
     g0 = _golden(name)
     dev = _cuda()
     m = _mech(mk["tables"])
