@@ -55,6 +55,8 @@ extern "C" {
 #define HC_RATE_TROE3 3
 #define HC_RATE_TROE4 4
 #define HC_RATE_SRI 5       /* fall-off with the SRI function (fallOffFunctions::SRI) */
+#define HC_RATE_PLOG 6      /* pressure-dependent Arrhenius table with logarithmic
+                               interpolation, Chemkin PLOG (logInterpolationRR) */
 
 /* hc_mech_desc.reversible */
 #define HC_IRREVERSIBLE 0
@@ -100,6 +102,12 @@ typedef struct hc_mech_desc {
     const double *sri;       /* [nrc*5] SRI a, b, c, d, e (HC_RATE_SRI reactions) */
     const double *arr_rev;   /* [nrc*3] reverse A, beta, Ta (HC_REVERSIBLE_REV reactions; for a
                                 third-body reaction the reverse rate is M times this) */
+    /* PLOG tables: entries plog_ptr[r] .. plog_ptr[r+1]-1 of reaction r, sorted by
+       pressure (equal pressures keep their file order and their rates add), the
+       two highest pressures distinct; NULL when no reaction is HC_RATE_PLOG */
+    const int32_t *plog_ptr; /* [nrc+1] */
+    const double *plog_p;    /* [plog_ptr[nrc]] pressures, Pa */
+    const double *plog_arr;  /* [plog_ptr[nrc]*3] A, beta, Ta of each entry */
 } hc_mech_desc;
 
 /*

@@ -36,6 +36,16 @@ def _arr_rev(t):
     return np.zeros((t.nrc, 3)) if a is None else a
 
 
+def _plog(t):
+    """PLOG tables (ptr [nrc+1], p [n], arr [n, 3]); empty for tables without them.
+    The arrays are never empty, so that their addresses are valid."""
+    ptr = getattr(t, "plog_ptr", None)
+    if ptr is None:
+        return np.zeros(t.nrc + 1, np.int32), np.zeros(1), np.zeros((1, 3))
+    return (ptr, t.plog_p if len(t.plog_p) else np.zeros(1),
+            t.plog_arr if len(t.plog_arr) else np.zeros((1, 3)))
+
+
 class HcMechDesc(C.Structure):
     _fields_ = [
         ("nsp", C.c_int32), ("nrc", C.c_int32),
@@ -46,6 +56,7 @@ class HcMechDesc(C.Structure):
         ("fnu", C.c_void_p), ("bnu", C.c_void_p), ("ford", C.c_void_p), ("bord", C.c_void_p),
         ("geom", C.c_void_p), ("eps_k", C.c_void_p), ("sigma", C.c_void_p),
         ("sri", C.c_void_p), ("arr_rev", C.c_void_p),
+        ("plog_ptr", C.c_void_p), ("plog_p", C.c_void_p), ("plog_arr", C.c_void_p),
     ]
 
 
@@ -182,7 +193,8 @@ class DescArrays:
             arr0=f64(t.arr0), troe=f64(t.troe), eff=f64(t.eff), nf=i32(t.nf), nb=i32(t.nb),
             fidx=i32(t.fidx), bidx=i32(t.bidx), fnu=f64(t.fnu), bnu=f64(t.bnu),
             ford=f64(t.ford), bord=f64(t.bord), geom=i32(t.geom), eps_k=f64(t.eps_k),
-            sigma=f64(t.sigma), sri=f64(_sri(t)), arr_rev=f64(_arr_rev(t)))
+            sigma=f64(t.sigma), sri=f64(_sri(t)), arr_rev=f64(_arr_rev(t)),
+            plog_ptr=i32(_plog(t)[0]), plog_p=f64(_plog(t)[1]), plog_arr=f64(_plog(t)[2]))
         d = HcMechDesc()
         d.nsp, d.nrc = int(t.nsp), int(t.nrc)
         for k, a in self.arrays.items():

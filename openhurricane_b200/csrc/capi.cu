@@ -196,7 +196,23 @@ static void make_host(const hc_mech_desc *d, HostMech &h) {
     h.arr_rev = permute(d->arr_rev ? d->arr_rev : zeros3.data(), 3);
     h.ext = false;
     for (int r = 0; r < nrc; ++r)
-        if (d->rate_type[r] == HC_RATE_SRI || d->reversible[r] == HC_REVERSIBLE_REV) h.ext = true;
+        if (d->rate_type[r] == HC_RATE_SRI || d->rate_type[r] == HC_RATE_PLOG ||
+            d->reversible[r] == HC_REVERSIBLE_REV)
+            h.ext = true;
+    // PLOG tables follow their reactions into device order
+    h.plog_ptr.assign((size_t)nrc + 1, 0);
+    h.plog_p.clear();
+    h.plog_arr.clear();
+    for (int r = 0; r < nrc; ++r) {
+        const int src = perm[r];
+        if (d->plog_ptr && d->rate_type[src] == HC_RATE_PLOG) {
+            for (int k = d->plog_ptr[src]; k < d->plog_ptr[src + 1]; ++k) {
+                h.plog_p.push_back(d->plog_p[k]);
+                for (int j = 0; j < 3; ++j) h.plog_arr.push_back(d->plog_arr[3 * (size_t)k + j]);
+            }
+        }
+        h.plog_ptr[r + 1] = (int32_t)h.plog_p.size();
+    }
     h.sum_stoi.assign(nrc, 0.0);
     for (int r = 0; r < nrc; ++r) {
         double s = 0.0;
@@ -267,12 +283,29 @@ static int check_desc(const hc_mech_desc *d) {
     for (int r = 0; r < nrc; ++r) {
         if (d->nf[r] < 0 || d->nf[r] > HC_MAX_SIDE || d->nb[r] < 0 || d->nb[r] > HC_MAX_SIDE)
             return fail(HC_E_INVALID, "reaction side larger than HC_MAX_SIDE");
-        if (d->rate_type[r] < 0 || d->rate_type[r] > HC_RATE_SRI)
+        if (d->rate_type[r] < 0 || d->rate_type[r] > HC_RATE_PLOG)
             return fail(HC_E_INVALID, "unknown rate type");
         if (d->reversible[r] < HC_IRREVERSIBLE || d->reversible[r] > HC_REVERSIBLE_REV)
             return fail(HC_E_INVALID, "unknown reversibility code");
         if (d->rate_type[r] == HC_RATE_SRI && !d->sri)
             return fail(HC_E_INVALID, "SRI reaction without SRI parameters");
+        if (d->rate_type[r] == HC_RATE_PLOG) {
+            if (!d->plog_ptr || !d->plog_p || !d->plog_arr)
+                return fail(HC_E_INVALID, "PLOG reaction without PLOG tables");
+            const int b = d->plog_ptr[r], e = d->plog_ptr[r + 1];
+            if (b < 0 || e <= b) return fail(HC_E_INVALID, "PLOG reaction with an empty table");
+            for (int k = b; k < e; ++k) {
+                if (!(d->plog_p[k] > 0)) return fail(HC_E_INVALID, "PLOG pressure not positive");
+                if (k > b && d->plog_p[k] < d->plog_p[k - 1])
+                    return fail(HC_E_INVALID, "PLOG pressures not sorted");
+            }
+            // logInterpolationRR::DkDT reads past its list for a repeated
+            // highest pressure (logInterpolationRR.cpp:170-179)
+            if (e - b > 1 && d->plog_p[e - 1] == d->plog_p[e - 2])
+                return fail(HC_E_INVALID, "PLOG table with its highest pressure twice");
+            if (d->reversible[r] == HC_REVERSIBLE_REV)
+                return fail(HC_E_INVALID, "explicit reverse parameters on a PLOG reaction");
+        }
         if (d->reversible[r] == HC_REVERSIBLE_REV) {
             if (!d->arr_rev) return fail(HC_E_INVALID, "REV reaction without reverse parameters");
             // reversibleReactionWithRevPars takes Arrhenius and third-body rates only
@@ -363,6 +396,7 @@ int hc_mech_create(const hc_mech_desc *d, hc_mech_t *out) {
     DevMech &dm = m->dm;
     dm.nsp = nsp;
     dm.nrc = nrc;
+    dm.ext = hm.ext ? 1 : 0;
     int rc = HC_OK;
     auto up = [&](auto *src, size_t n, auto **dst) {
         if (rc == HC_OK) rc = upload(m->owned, src, n, dst);
@@ -377,6 +411,9 @@ int hc_mech_create(const hc_mech_desc *d, hc_mech_t *out) {
     up(p_troe.data(), 4 * (size_t)nrc, &dm.troe);
     up(hm.sri.data(), 5 * (size_t)nrc, &dm.sri);
     up(hm.arr_rev.data(), 3 * (size_t)nrc, &dm.arr_rev);
+    up(hm.plog_ptr.data(), (size_t)nrc + 1, &dm.plog_ptr);
+    up(hm.plog_p.data(), hm.plog_p.size(), &dm.plog_p);
+    up(hm.plog_arr.data(), hm.plog_arr.size(), &dm.plog_arr);
     up(p_eff.data(), (size_t)nrc * nsp, &dm.eff);
     up(p_nf.data(), nrc, &dm.nf);
     up(p_nb.data(), nrc, &dm.nb);
@@ -481,7 +518,7 @@ int hc_jit_source(const hc_mech_desc *d, int block, char *buf, int64_t cap, int6
     make_host(d, h);
     if (h.ext)
         return fail(HC_E_UNSUPPORTED,
-                    "no generated kernel for SRI or explicit reverse (REV) rate laws");
+                    "no generated kernel for SRI, explicit reverse (REV) or PLOG rate laws");
     const std::string src = jit_t1_source(h, block);
     *len = (int64_t)src.size();
     if (buf && cap > 0) {
@@ -544,11 +581,11 @@ static int integrate_impl(hc_mech_t m, const hc_opts *opts, int64_t ncells, doub
     if (m->kernel == 1 && !t1_ok)
         return fail(HC_E_UNSUPPORTED,
                     "thread-per-cell kernel needs nsp <= 15, autoUpdateJacobian off and no SRI "
-                    "or explicit reverse (REV) rate laws");
+                    "or explicit reverse (REV) rate laws or PLOG tables");
     if (m->kernel == 4 && !(t1_ok && m->t2_ok))
         return fail(HC_E_UNSUPPORTED,
                     "compact thread-per-cell kernel needs nsp <= 15, <= 64 reactions, "
-                    "autoUpdateJacobian off and no SRI or explicit reverse (REV) rate laws");
+                    "autoUpdateJacobian off and no SRI, explicit reverse (REV) or PLOG rate laws");
     // automatic choice: the cell group. Per-cell costs in a flow step differ
     // by orders of magnitude, and the step lasts as long as its stiffest
     // cell; the cell group's lanes share each Newton iteration's work and
@@ -572,7 +609,7 @@ static int integrate_impl(hc_mech_t m, const hc_opts *opts, int64_t ncells, doub
     if (m->kernel == 3 && !t1_ok)
         return fail(HC_E_UNSUPPORTED,
                     "generated thread-per-cell kernel needs nsp <= 15, autoUpdateJacobian off and "
-                    "no SRI or explicit reverse (REV) rate laws");
+                    "no SRI, explicit reverse (REV) or PLOG rate laws");
     bool use_jit = t1_ok && m->kernel == 3;
     if (use_jit && !m->jit_tried) {
         // first use: generate, compile and load (host work, no stream operation)
@@ -1140,7 +1177,7 @@ extern "C" int hc_integrate_noalloc(hc_mech_t m, const hc_opts *opts, int64_t nc
     if (N > 16 || opts->auto_update_jacobian || !m->t2_ok)
         return fail(HC_E_UNSUPPORTED,
                     "hc_integrate_noalloc needs nsp <= 15, <= 64 reactions, autoUpdateJacobian off "
-                    "and no SRI or explicit reverse (REV) rate laws");
+                    "and no SRI, explicit reverse (REV) or PLOG rate laws");
     int dev = -1;
     HC_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 256) return fail(HC_E_CUDA, "device ordinal out of range");

@@ -64,7 +64,11 @@ struct Smem {
     static constexpr int kSize = kRedI + 4;                 // doubles
 };
 
-template <int N, int G>
+// X: the mechanism may use the rate forms only some mechanisms need (SRI
+// fall-off, explicit reverse parameters, PLOG tables). The integrator is
+// instantiated with and without them and launched without them when the
+// mechanism has none, so that their branches cost the common forms nothing.
+template <int N, int G, bool X = true>
 struct CellCtx {
     const DevMech &m;
     const IntegratorParams &P;
@@ -173,7 +177,7 @@ struct CellCtx {
             bo[k] = (k < nb) ? ldg(&m.bord[kMaxSide * r + k]) : 0.0;
         }
         double M = 0.0;
-        if (type != kArrhenius) {
+        if (type != kArrhenius && !(X && type == kPLOG)) {
             const double *e = &m.eff[(int64_t)r * nsp];
             for (int i = 0; i < nsp; ++i) M += ldg(&e[i]) * c[i];
         }
@@ -183,6 +187,8 @@ struct CellCtx {
             kf = arrK_log(A, b, Ta, T, logT);
         } else if (type == kThirdBody) {
             kf = M * arrK_log(A, b, Ta, T, logT);
+        } else if (X && type == kPLOG) {
+            kf = plog_k_global(m.plog_ptr, m.plog_p, m.plog_arr, r, p, T, logT);
         } else {
             const double A0 = ldg(&m.arr0[3 * r]);
             b0 = ldg(&m.arr0[3 * r + 1]);
@@ -190,7 +196,7 @@ struct CellCtx {
             k0 = arrK_log(A0, b0, Ta0, T, logT);
             kinf = arrK_log(A, b, Ta, T, logT);
             Pr = k0 / notZeroD(kinf) * M;
-            if (type == kSRI) {
+            if (X && type == kSRI) {
                 F = sri_F_global(&m.sri[5 * r], T, Pr);
             } else {
                 if (type != kLindemann) lf = troe_logfcent(&m.troe[4 * r], type == kTroe4, T);
@@ -201,7 +207,7 @@ struct CellCtx {
         double kr = 0.0, Kc = 0.0, DKcDT = 0.0;
         const int rev_kind = ldg(&m.reversible[r]);
         const bool rev = rev_kind != 0;
-        if (rev_kind == kRevExplicit) {
+        if (X && rev_kind == kRevExplicit) {
             // reversibleReactionWithRevPars::kr (reversibleReactionWithRevPars.hpp:68-76):
             // the reverse rate law of the same kind, M times it for third-body
             kr = arr_global(&m.arr_rev[3 * r], T, logT);
@@ -278,11 +284,13 @@ struct CellCtx {
         double dkfdT;
         if (type == kArrhenius || type == kThirdBody) {
             dkfdT = kf * invT * (b + Ta * invT);
+        } else if (X && type == kPLOG) {
+            dkfdT = plog_dkdt_global(m.plog_ptr, m.plog_p, m.plog_arr, r, kf, p, T, logT);
         } else {
             dkfdT = (Pr / (1.0 + Pr)) * F * (kinf * invT * (b + Ta * invT));
         }
         double dkrdT = 0.0;
-        if (rev_kind == kRevExplicit)
+        if (X && rev_kind == kRevExplicit)
             dkrdT = kr * invT * (ldg(&m.arr_rev[3 * r + 1]) + ldg(&m.arr_rev[3 * r + 2]) * invT);
         else if (rev) dkrdT = (dkfdT - kr * DKcDT) / hmax(Kc, kVeryTiny);
 #pragma unroll
@@ -301,19 +309,19 @@ struct CellCtx {
         if (type == kThirdBody) {
             kind = 1.0;
             rec[11] = q / hmax(M, kTiny);
-        } else if (type != kArrhenius) {
+        } else if (type != kArrhenius && !(X && type == kPLOG)) {
             if (M > kTiny) {
                 // unimolecularFallOffRR::gamDGamDT (unimolecularFallOffRR.cpp:55-91)
                 const double Pr2 = k0 * M / notZeroD(kinf);
                 const double F2 =
-                    (type == kSRI) ? sri_F_global(&m.sri[5 * r], T, Pr2) : fall_F(type, lf, Pr2);
+                    (X && type == kSRI) ? sri_F_global(&m.sri[5 * r], T, Pr2) : fall_F(type, lf, Pr2);
                 const double dPrdT = Pr2 * ((k0 * invT * (b0 + Ta0 * invT)) / notZeroD(k0) -
                                             (kinf * invT * (b + Ta * invT)) / notZeroD(kinf));
-                const double dFdT = (type == kSRI)
+                const double dFdT = (X && type == kSRI)
                                         ? sri_dfdt_global(&m.sri[5 * r], T, Pr2, F2, dPrdT)
                                         : troe_dfdt(type, &m.troe[4 * r], T, Pr2, F2, dPrdT);
                 dgdT = q * (dPrdT / (Pr2 * (1 + Pr2)) + dFdT / F2);
-                const double fabc = (type == kSRI)
+                const double fabc = (X && type == kSRI)
                                         ? sri_dfdci_factor_global(&m.sri[5 * r], T, Pr2, F2)
                                         : troe_dfdci_factor(type, lf, Pr2, F2);
                 const double g = q * (k0 / notZeroD(kinf)) *
@@ -449,9 +457,9 @@ struct CellCtx {
 
 enum CellRc : int { kRcOk = 0, kRcUnderflow = 1, kRcIterLimit = 2 };
 
-template <int N, int G>
-struct CellIntegrator : CellCtx<N, G> {
-    using Base = CellCtx<N, G>;
+template <int N, int G, bool X = true>
+struct CellIntegrator : CellCtx<N, G, X> {
+    using Base = CellCtx<N, G, X>;
     using Base::g;
     using Base::P;
     using Base::nsp;
@@ -673,7 +681,7 @@ __device__ __forceinline__ Group<G> make_group(double *s, int gid, int red_off, 
 // evaluation-only kernels use no integrator option
 __device__ const IntegratorParams kNoParams{};
 
-template <int N, int G>
+template <int N, int G, bool X = true>
 #ifndef HC_GROUP_MIN_BLOCKS
 #define HC_GROUP_MIN_BLOCKS 4   // blocks of 128 threads per SM the 32-lane groups are built for (measured best)
 #endif
@@ -698,7 +706,7 @@ integrate_kernel(const __grid_constant__ DevMech m, const __grid_constant__ Inte
         g.sync();
         if (k >= io.nqueue) break;
         const int64_t cell = io.order ? (int64_t)io.order[k] : (int64_t)k;
-        CellIntegrator<N, G> ci(m, P, g, s);
+        CellIntegrator<N, G, X> ci(m, P, g, s);
         const double Ti = io.T[cell];
         const double tstep = io.dt[cell] * io.dt_factor;
         const double rho0 = io.rho[cell];

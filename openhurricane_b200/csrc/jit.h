@@ -19,8 +19,10 @@ struct HostMech {
     std::vector<int32_t> rate_type, reversible, nf, nb, fidx, bidx;
     std::vector<double> arr, arr0, troe, eff, fnu, bnu, ford, bord, sum_stoi;
     std::vector<double> sri, arr_rev;
+    std::vector<int32_t> plog_ptr;         // [nrc+1], in device reaction order
+    std::vector<double> plog_p, plog_arr;
     // the mechanism uses rate forms only the cell-group kernels evaluate
-    // (SRI fall-off, explicit reverse parameters)
+    // (SRI fall-off, explicit reverse parameters, PLOG tables)
     bool ext = false;
 };
 

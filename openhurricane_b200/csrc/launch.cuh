@@ -27,7 +27,8 @@ struct Launch {
 
     static int integrate(const DevMech &m, int num_sms, const IntegratorParams &P,
                          const CellIO &io, cudaStream_t st, std::string &err) {
-        auto kern = integrate_kernel<N, G>;
+        // the instantiation without the rarer rate forms unless the mechanism has them
+        auto kern = m.ext ? integrate_kernel<N, G, true> : integrate_kernel<N, G, false>;
         const size_t sm = smem_bytes();
         HC_LCUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         int per_sm = 0;

@@ -20,6 +20,9 @@ struct DevMech {
     const int32_t *rate_type, *reversible;
     const double *arr, *arr0, *troe;  // [nrc*3], [nrc*3], [nrc*4]
     const double *sri, *arr_rev;      // [nrc*5] SRI a..e, [nrc*3] explicit reverse Arrhenius
+    int32_t ext;                      // any SRI, REV or PLOG reaction
+    const int32_t *plog_ptr;          // [nrc+1] PLOG entries of each reaction
+    const double *plog_p, *plog_arr;  // [n] Pa, [n*3] A, beta, Ta
     const double *eff;      // [nrc*nsp]
     const int32_t *nf, *nb; // [nrc]
     const int32_t *fidx, *bidx;       // [nrc*4]
@@ -119,6 +122,20 @@ static __device__ __noinline__ double sri_dfdci_factor_global(const double *s, d
                                                        double F) {
     const double p[5] = {ldg(&s[0]), ldg(&s[1]), ldg(&s[2]), ldg(&s[3]), ldg(&s[4])};
     return sri_dfdci_factor(p, T, Pr, F);
+}
+
+static __device__ __noinline__ double plog_k_global(const int32_t *ptr, const double *pp,
+                                                   const double *pa, int r, double p, double T,
+                                                   double logT) {
+    const int b = ldg(&ptr[r]), n = ldg(&ptr[r + 1]) - b;
+    return plog_k(&pp[b], &pa[3 * b], n, p, T, logT);
+}
+
+static __device__ __noinline__ double plog_dkdt_global(const int32_t *ptr, const double *pp,
+                                                      const double *pa, int r, double kj,
+                                                      double p, double T, double logT) {
+    const int b = ldg(&ptr[r]), n = ldg(&ptr[r + 1]) - b;
+    return plog_dkdt(&pp[b], &pa[3 * b], n, kj, p, T, logT);
 }
 
 static __device__ __noinline__ double arr_global(const double *a, double T, double logT) {

@@ -26,7 +26,7 @@ constexpr double kRu = (1.380649e-23 * 6.02214076e23) * 1e3;
 constexpr int kMaxSide = 4;
 
 enum RateType : int32_t {
-    kArrhenius = 0, kThirdBody = 1, kLindemann = 2, kTroe3 = 3, kTroe4 = 4, kSRI = 5
+    kArrhenius = 0, kThirdBody = 1, kLindemann = 2, kTroe3 = 3, kTroe4 = 4, kSRI = 5, kPLOG = 6
 };
 // reversible flags: 1 kr = kf / Kc, 2 kr from explicit reverse Arrhenius parameters
 constexpr int32_t kRevExplicit = 2;
@@ -161,6 +161,74 @@ __device__ __forceinline__ double sri_dfdt(const double *s, double T, double Pr,
     const double base = s[0] * eb + ec;
     return F * (s[4] / T + dXdPr * DPrDT * log(base) +
                 X * (s[0] * s[1] * eb / (T * T) - ec / s[2]) / base);
+}
+
+// PLOG (logInterpolationRR::k and ::DkDT, logInterpolationRR.cpp:78-147,
+// 149-226) over one reaction's table: pressures pp[n] (Pa, sorted, the two
+// highest distinct) and Arrhenius entries pa[3n]. Below the table the rates
+// of the entries at the lowest pressure add, above it the highest entry is
+// taken; inside, the reference's loop over intervals does not stop at the
+// first that brackets p, so the interval it evaluates last -- the two
+// highest pressures, with the entries sharing the lower of them added --
+// is the one used, interpolated (or extrapolated) in ln p.
+__device__ __forceinline__ double plog_entry_dkdt(const double *a, double kj, double T) {
+    const double invT = 1.0 / hmax(T, kTiny);
+    return kj * invT * (a[1] + a[2] * invT);
+}
+
+__device__ __forceinline__ double plog_k(const double *pp, const double *pa, int n, double p,
+                                         double T, double logT) {
+    if (p <= pp[0]) {
+        double k = arrK_log(pa[0], pa[1], pa[2], T, logT);
+        for (int i = 0; i < n - 1; ++i) {
+            if (pp[i + 1] > pp[i]) break;
+            k += arrK_log(pa[3 * (i + 1)], pa[3 * (i + 1) + 1], pa[3 * (i + 1) + 2], T, logT);
+        }
+        return k;
+    }
+    if (p >= pp[n - 1]) return arrK_log(pa[3 * (n - 1)], pa[3 * (n - 1) + 1], pa[3 * (n - 1) + 2], T, logT);
+    const int i = n - 2;
+    double k0 = arrK_log(pa[3 * i], pa[3 * i + 1], pa[3 * i + 2], T, logT);
+    for (int j = i - 1; j >= 0; --j) {
+        if (pp[j + 1] > pp[j]) break;
+        k0 += arrK_log(pa[3 * j], pa[3 * j + 1], pa[3 * j + 2], T, logT);
+    }
+    const double k1 = arrK_log(pa[3 * (i + 1)], pa[3 * (i + 1) + 1], pa[3 * (i + 1) + 2], T, logT);
+    const double lnk0 = log(k0), lnk1 = log(k1);
+    const double lnp0 = log(pp[i]), lnp1 = log(pp[i + 1]), lnp = log(p);
+    return exp(lnk0 + (lnk1 - lnk0) * (lnp - lnp0) / (lnp1 - lnp0));
+}
+
+__device__ __forceinline__ double plog_dkdt(const double *pp, const double *pa, int n, double kj,
+                                            double p, double T, double logT) {
+    if (p <= pp[0]) {
+        double d = plog_entry_dkdt(&pa[0], arrK_log(pa[0], pa[1], pa[2], T, logT), T);
+        for (int i = 0; i < n - 1; ++i) {
+            if (pp[i + 1] > pp[i]) break;
+            const double *a = &pa[3 * (i + 1)];
+            d += plog_entry_dkdt(a, arrK_log(a[0], a[1], a[2], T, logT), T);
+        }
+        return d;
+    }
+    if (p >= pp[n - 1]) {
+        const double *a = &pa[3 * (n - 1)];
+        return plog_entry_dkdt(a, arrK_log(a[0], a[1], a[2], T, logT), T);
+    }
+    const int i = n - 2;
+    double k0 = arrK_log(pa[3 * i], pa[3 * i + 1], pa[3 * i + 2], T, logT);
+    double dk0 = plog_entry_dkdt(&pa[3 * i], k0, T);
+    for (int j = i - 1; j >= 0; --j) {
+        if (pp[j + 1] > pp[j]) break;
+        const double kj0 = arrK_log(pa[3 * j], pa[3 * j + 1], pa[3 * j + 2], T, logT);
+        k0 += kj0;
+        dk0 += plog_entry_dkdt(&pa[3 * j], kj0, T);
+    }
+    const double *a1 = &pa[3 * (i + 1)];
+    const double k1 = arrK_log(a1[0], a1[1], a1[2], T, logT);
+    const double dk1 = plog_entry_dkdt(a1, k1, T);
+    const double lnp0 = log(pp[i]), lnp1 = log(pp[i + 1]), lnp = log(p);
+    const double dlnkdT = 1.0 / k0 * dk0 + (1.0 / k1 * dk1 - 1.0 / k0 * dk0) * (lnp - lnp0) / (lnp1 - lnp0);
+    return kj * dlnkdT;
 }
 
 struct IntegratorParams {

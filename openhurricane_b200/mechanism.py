@@ -35,8 +35,9 @@ fall-off (+M) with Lindemann, Troe (3 or 4 parameters) or SRI (3 or 5
 parameters); reversible (=, <=>) and irreversible (=>) reactions; explicit
 reverse Arrhenius parameters (REV, reversibleReactionWithRevPars) on
 Arrhenius and third-body reactions; non-stoichiometric orders (FORD, RORD).
-The reference's other rate forms (PLOG, CHEB, HIGH, LT, JAN, ...) are
-rejected with NotImplementedError.
+pressure-dependent Arrhenius tables (PLOG, logInterpolationRR) on reactions
+without a third body. The reference's other rate forms (CHEB, HIGH, LT,
+JAN, ...) are rejected with NotImplementedError.
 """
 from __future__ import annotations
 
@@ -72,6 +73,7 @@ RATE_LINDEMANN = 2
 RATE_TROE3 = 3
 RATE_TROE4 = 4
 RATE_SRI = 5
+RATE_PLOG = 6
 
 # reversibility codes
 IRREVERSIBLE = 0
@@ -86,7 +88,7 @@ UNITS_E = {"CAL": "CAL", "CAL/MOLE": "CAL", "EVOL": "EVOL", "EVOLTS": "EVOL", "J
            "KELVINS": "KELV", "KJOU": "KJOU", "KJOULES/MOLE": "KJOU"}
 ELECTRON_VOLT = 1.6021766208e-19    # J (physicalConstant.hpp:59,114)
 # auxiliary keywords of the reference's reader that this reader does not take
-_UNSUPPORTED_AUX = {"PLOG", "CHEB", "PCHEB", "TCHEB", "HIGH", "LT", "RLT", "JAN", "FIT1", "TDEP",
+_UNSUPPORTED_AUX = {"CHEB", "PCHEB", "TCHEB", "HIGH", "LT", "RLT", "JAN", "FIT1", "TDEP",
                     "XSMI", "MOME", "EXCI", "COLLEFF"}
 
 
@@ -108,6 +110,7 @@ class ParsedReaction:
     rord: Optional[Dict[int, float]] = None     # species -> reverse order (RORD)
     units_A: str = "MOLES"
     units_E: str = "CAL"
+    plog: Optional[List[Tuple[float, float, float, float]]] = None   # (p atm, A, b, E) as read
 
 
 @dataclasses.dataclass
@@ -144,6 +147,9 @@ class MechTables:
     zrot: np.ndarray
     sri: Optional[np.ndarray] = None       # [nrc, 5] a, b, c, d, e (SRI fall-off)
     arr_rev: Optional[np.ndarray] = None   # [nrc, 3] explicit reverse A, beta, Ta (REV)
+    plog_ptr: Optional[np.ndarray] = None  # [nrc + 1] int32 entries of each PLOG reaction
+    plog_p: Optional[np.ndarray] = None    # [n] Pa, sorted per reaction
+    plog_arr: Optional[np.ndarray] = None  # [n, 3] A, beta, Ta
 
     @property
     def nsp(self) -> int:
@@ -284,6 +290,15 @@ def parse_chemkin(che_text: str, species_names: Optional[List[str]] = None):
                 if len(v) not in (3, 5):
                     raise ValueError("SRI takes 3 or 5 parameters")
                 cur.sri = [_read_real(x) for x in v]
+            elif up == "PLOG":
+                # chemkinFileRead.cpp:606-644: PLOG / p[atm] A b E /, not with a third body
+                if cur.kind != "arrhenius":
+                    raise ValueError("PLOG cannot be used on a third-body or fall-off reaction")
+                if len(v) != 4:
+                    raise ValueError("PLOG takes a pressure and three Arrhenius parameters")
+                if cur.plog is None:
+                    cur.plog = []
+                cur.plog.append(tuple(_read_real(x) for x in v))
             elif up == "REV":
                 cur.rev = (_read_real(v[0]), _read_real(v[1]), _read_real(v[2]))
             elif up in ("FORD", "RORD"):
@@ -420,6 +435,7 @@ def compile_mechanism(che_path: str, thermo_path: str, transport_path: str) -> M
     ford = np.zeros((nrc, MAX_SIDE))
     bord = np.zeros((nrc, MAX_SIDE))
     sum_stoi = np.zeros(nrc)
+    plog_rows = []
     for r, rx in enumerate(reactions):
         if len(rx.fwd) > MAX_SIDE or len(rx.bwd) > MAX_SIDE:
             raise ValueError("too many species on one side")
@@ -432,7 +448,21 @@ def compile_mechanism(che_path: str, thermo_path: str, transport_path: str) -> M
             order += o
         third = rx.kind != "arrhenius"
         Afac, Efac = change_unit(order, rx.units_A, rx.units_E, third)
-        if rx.kind == "arrhenius":
+        if rx.plog is not None:
+            if rx.rev is not None:
+                raise ValueError("REV cannot be used with a PLOG rate (chemkinFileRead.cpp:1609)")
+            # logInterpolationRR::append sorts by pressure after each entry
+            # (a stable bubble sort, logInterpolationRR.cpp:37-60); the
+            # pressures then become Pa and each entry takes the reaction's
+            # unit factors (chemkinFileRead.cpp:1596-1603)
+            ent = sorted(rx.plog, key=lambda e: e[0])
+            if len(ent) > 1 and ent[-1][0] == ent[-2][0]:
+                raise ValueError("PLOG table with its highest pressure twice: the reference's "
+                                 "derivative reads past its table there")
+            rate_type[r] = RATE_PLOG
+            arr[r] = (rx.A * Afac, rx.b, rx.E / Efac)
+            plog_rows.append((r, [(pa * PATM, A_ * Afac, b_, E_ / Efac) for pa, A_, b_, E_ in ent]))
+        elif rx.kind == "arrhenius":
             rate_type[r] = RATE_ARRHENIUS
             arr[r] = (rx.A * Afac, rx.b, rx.E / Efac)
         elif rx.kind == "third_body":
@@ -482,6 +512,18 @@ def compile_mechanism(che_path: str, thermo_path: str, transport_path: str) -> M
             s += nu
         sum_stoi[r] = s
 
+    plog_ptr = np.zeros(nrc + 1, np.int32)
+    counts = np.zeros(nrc, np.int64)
+    for r, ent in plog_rows:
+        counts[r] = len(ent)
+    plog_ptr[1:] = np.cumsum(counts)
+    plog_p = np.zeros(int(plog_ptr[-1]))
+    plog_arr = np.zeros((int(plog_ptr[-1]), 3))
+    for r, ent in plog_rows:
+        for k, (pa, A_, b_, Ta_) in enumerate(ent):
+            plog_p[plog_ptr[r] + k] = pa
+            plog_arr[plog_ptr[r] + k] = (A_, b_, Ta_)
+
     geom = np.zeros(nsp, np.int32)
     eps = np.ones(nsp)
     sig = np.ones(nsp)
@@ -494,7 +536,8 @@ def compile_mechanism(che_path: str, thermo_path: str, transport_path: str) -> M
             geom[i], eps[i], sig[i], dip[i], pol[i], zr[i] = g, e_, s_, d_, p_, z_
     return MechTables(names, W, Ri, Tr, nasa, el_names, E, rate_type, rev, arr, arr0, troe,
                       eff, nf, nb, fidx, bidx, fnu, bnu, ford, bord, sum_stoi,
-                      geom, eps, sig, dip, pol, zr, sri=sri, arr_rev=arr_rev)
+                      geom, eps, sig, dip, pol, zr, sri=sri, arr_rev=arr_rev,
+                      plog_ptr=plog_ptr, plog_p=plog_p, plog_arr=plog_arr)
 
 
 def element_matrix_mass(m: MechTables) -> np.ndarray:

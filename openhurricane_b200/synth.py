@@ -68,6 +68,8 @@ class Reaction:
     ford: Dict[str, float] = dataclasses.field(default_factory=dict)
     rord: Dict[str, float] = dataclasses.field(default_factory=dict)
     units: Optional[str] = None                        # UNITS /.../ of this reaction
+    plog: List[Tuple[float, float, float, float]] = dataclasses.field(default_factory=list)
+    #                                                  # PLOG p [atm], A, b, Ea (cal/mol)
 
 
 @dataclasses.dataclass
@@ -319,7 +321,8 @@ def extended_mechanism(seed: int = 20241117) -> Mechanism:
     one Troe, explicit reverse parameters (REV) on two Arrhenius and one
     third-body reaction, a forward and a reverse order override (FORD 1.5,
     RORD 1.5), energies written in kJ/mol on the REACTIONS line, and
-    per-reaction UNITS (molecules for one reaction, kcal/mol for another).
+    per-reaction UNITS (molecules for one reaction, kcal/mol for another),
+    and three PLOG pressure tables.
     The rate parameters stay those of the drawn mechanism; the file carries
     them in the declared units. (Orders below one give rates that are not
     Lipschitz at zero concentration; with such an order this mechanism's
@@ -353,6 +356,14 @@ def extended_mechanism(seed: int = 20241117) -> Mechanism:
     plain[3].rord = {plain[3].products[0][0]: 1.5}
     plain[4].units = "MOLEC"
     plain[5].units = "KCAL"
+    # pressure tables: cells at 1-5 atm fall inside the first (interpolated),
+    # above the second and below the third (whose lowest pressure is listed
+    # twice, the two rates adding up)
+    for r, ps in ((plain[6], (0.1, 1.0, 10.0)), (plain[7], (0.01, 0.1, 0.5)),
+                  (plain[8], (10.0, 10.0, 100.0))):
+        r.plog = [(pa, float(r.A * 10.0 ** rng.uniform(-1.0, 1.0)),
+                   float(np.round(r.b + rng.uniform(-0.2, 0.2), 6)),
+                   float(np.round(r.Ea + rng.uniform(-2000.0, 2000.0), 4))) for pa in ps]
     return m
 
 
@@ -451,6 +462,8 @@ def write_chemkin(mech: Mechanism, out_dir: str, stem: str = "mech") -> Tuple[st
             lines.append(f"   RORD / {k} {v:g} /")
         if r.units:
             lines.append(f"   UNITS / {r.units} /")
+        for pa, Ap, bp, Ep in r.plog:
+            lines.append(f"   PLOG / {pa:g}  {A(Ap, fo):.6E}  {bp:.6f}  {E(Ep):.4f} /")
     lines += ["END", ""]
     with open(che, "w") as f:
         f.write("\n".join(lines))

@@ -59,6 +59,7 @@ static inline double hmin(double a, double b) { return (b < a) ? b : a; }
 typedef struct {
     const hc_mech_desc *m;
     double *G0, *DG0DT;     /* [nsp] */
+    double p;               /* the cell's pressure (pressure-dependent rate tables) */
 } mech_ctx;
 
 /* ---------------- thermo (mass basis coefficients) ---------------- */
@@ -260,10 +261,112 @@ static double fallDFDT(const hc_mech_desc *m, int r, double T, double Pr, double
     return (F * ln10 * (DlogFcentDT / s1 - logFcent / (s1 * s1) * dPPDT));
 }
 
-static double rateK(const hc_mech_desc *m, int r, double T, const double *c) {
+/* PLOG (logInterpolationRR.cpp:78-147 k, :149-226 DkDT): the entries of
+   reaction r sorted by pressure, equal pressures adding their rates. Restated
+   loop for loop: inside the table the loop over intervals does not stop at
+   the first one that brackets p, so the last interval (the two highest
+   pressures) is the one evaluated. At the top the reference adds duplicated
+   highest pressures, and its derivative indexes one past its list there;
+   tables with a duplicated highest pressure are rejected by the reader and
+   by hc_mech_create, so that branch only ever sees its first entry. */
+static double plogK(const hc_mech_desc *m, int r, double p, double T) {
+    const int b = m->plog_ptr[r], n = m->plog_ptr[r + 1] - b;
+    const double *pp = &m->plog_p[b], *pa = &m->plog_arr[3 * b];
+    double k = 0.0;
+    if (p <= pp[0]) {
+        k = arrK(&pa[0], T);
+        for (int i = 0; i < n - 1; i++) {
+            if (pp[i + 1] > pp[i]) break;
+            k += arrK(&pa[3 * (i + 1)], T);
+        }
+    } else if (p >= pp[n - 1]) {
+        k = arrK(&pa[3 * (n - 1)], T);
+        for (int i = n - 1; i > 1; i--) {
+            if (pp[i - 1] < pp[i]) break;
+            k += arrK(&pa[3 * (i - 1)], T);
+        }
+    } else {
+        for (int i = 0; i < n - 1; i++) {
+            if (p < pp[i + 1]) {
+                double k0 = arrK(&pa[3 * i], T);
+                for (int j = i - 1; j >= 0; j--) {
+                    if (pp[j + 1] > pp[j]) break;
+                    k0 += arrK(&pa[3 * j], T);
+                }
+                double k1 = arrK(&pa[3 * (i + 1)], T);
+                for (int j = i + 1; j < n - 1; j++) {
+                    if (pp[j + 1] > pp[j]) break;
+                    k1 += arrK(&pa[3 * (j + 1)], T);
+                }
+                const double lnk0 = log(k0);
+                const double lnk1 = log(k1);
+                const double lnp0 = log(pp[i]);
+                const double lnp1 = log(pp[i + 1]);
+                const double lnp = log(p);
+                const double lnk = lnk0 + (lnk1 - lnk0) * (lnp - lnp0) / (lnp1 - lnp0);
+                k = exp(lnk);
+            }
+        }
+    }
+    return k;
+}
+
+static double plogDkDT(const hc_mech_desc *m, int r, double kj, double p, double T) {
+    const int b = m->plog_ptr[r], n = m->plog_ptr[r + 1] - b;
+    const double *pp = &m->plog_p[b], *pa = &m->plog_arr[3 * b];
+    double dkdT = 0.0;
+    if (p <= pp[0]) {
+        const double k0 = arrK(&pa[0], T);
+        dkdT = arrDkDT(&pa[0], k0, T);
+        for (int i = 0; i < n - 1; i++) {
+            if (pp[i + 1] > pp[i]) break;
+            const double ki = arrK(&pa[3 * (i + 1)], T);
+            dkdT += arrDkDT(&pa[3 * (i + 1)], ki, T);
+        }
+    } else if (p >= pp[n - 1]) {
+        const double kl = arrK(&pa[3 * (n - 1)], T);
+        dkdT = arrDkDT(&pa[3 * (n - 1)], kl, T);
+        for (int i = n - 1; i > 1; i--) {
+            if (pp[i - 1] < pp[i]) break;
+            const double ki = arrK(&pa[3 * (i - 1)], T);
+            dkdT += arrDkDT(&pa[3 * (i - 1)], ki, T);
+        }
+    } else {
+        for (int i = 0; i < n - 1; i++) {
+            if (p < pp[i + 1]) {
+                double k0 = arrK(&pa[3 * i], T);
+                double dk0dT = arrDkDT(&pa[3 * i], k0, T);
+                for (int j = i - 1; j >= 0; j--) {
+                    if (pp[j + 1] > pp[j]) break;
+                    const double kj0 = arrK(&pa[3 * j], T);
+                    k0 += kj0;
+                    dk0dT += arrDkDT(&pa[3 * j], kj0, T);
+                }
+                double k1 = arrK(&pa[3 * (i + 1)], T);
+                double dk1dT = arrDkDT(&pa[3 * (i + 1)], k1, T);
+                for (int j = i + 1; j < n - 1; j++) {
+                    if (pp[j + 1] > pp[j]) break;
+                    const double kj1 = arrK(&pa[3 * (j + 1)], T);
+                    k1 += kj1;
+                    dk1dT += arrDkDT(&pa[3 * (j + 1)], kj1, T);
+                }
+                const double lnp0 = log(pp[i]);
+                const double lnp1 = log(pp[i + 1]);
+                const double lnp = log(p);
+                const double dlnkdT =
+                    1.0 / k0 * dk0dT + (1.0 / k1 * dk1dT - 1.0 / k0 * dk0dT) * (lnp - lnp0) / (lnp1 - lnp0);
+                dkdT = kj * dlnkdT;
+            }
+        }
+    }
+    return dkdT;
+}
+
+static double rateK(const hc_mech_desc *m, int r, double p, double T, const double *c) {
     const int t = m->rate_type[r];
     const double *a = &m->arr[3 * r];
     if (t == HC_RATE_ARRHENIUS) return arrK(a, T);
+    if (t == HC_RATE_PLOG) return plogK(m, r, p, T);
     if (t == HC_RATE_THIRD_BODY) {
         const double M = thirdM(m, r, c);
         return (M * arrK(a, T));
@@ -274,10 +377,12 @@ static double rateK(const hc_mech_desc *m, int r, double T, const double *c) {
     return kinf * (Pr / (1.0 + Pr)) * fallF(m, r, T, Pr);
 }
 
-static double rateDkDT(const hc_mech_desc *m, int r, double kj, double T, const double *c) {
+static double rateDkDT(const hc_mech_desc *m, int r, double kj, double p, double T,
+                       const double *c) {
     const int t = m->rate_type[r];
     const double *a = &m->arr[3 * r];
     if (t == HC_RATE_ARRHENIUS || t == HC_RATE_THIRD_BODY) return arrDkDT(a, kj, T);
+    if (t == HC_RATE_PLOG) return plogDkDT(m, r, kj, p, T);
     const double k0 = arrK(&m->arr0[3 * r], T);
     const double kinf = arrK(a, T);
     const double Pr = k0 / notZeroD(kinf) * thirdM(m, r, c);
@@ -311,7 +416,7 @@ static void gamDGamDCi(const hc_mech_desc *m, int r, double T, const double *c, 
 
 static double gamDGamDT(const hc_mech_desc *m, int r, double T, const double *c) {
     const int t = m->rate_type[r];
-    if (t == HC_RATE_ARRHENIUS || t == HC_RATE_THIRD_BODY) return 0.0;
+    if (t == HC_RATE_ARRHENIUS || t == HC_RATE_THIRD_BODY || t == HC_RATE_PLOG) return 0.0;
     const double M = thirdM(m, r, c);
     if (M > TINY) {
         const double *a0 = &m->arr0[3 * r], *a = &m->arr[3 * r];
@@ -411,7 +516,7 @@ static double DkrDT(const mech_ctx *x, int r, double kr, double T, double dkfdT)
 static double qRate(const mech_ctx *x, int r, double T, const double *c, double *dcdt, double *kfo,
                     double *kro) {
     const hc_mech_desc *m = x->m;
-    double qf = rateK(m, r, T, c);
+    double qf = rateK(m, r, x->p, T, c);
     if (kfo) *kfo = qf;
     double qr = kRev(x, r, qf, T, c);
     if (kro) *kro = qr;
@@ -469,7 +574,7 @@ static void DqDci(const mech_ctx *x, int r, double kf, double kr, double qfr, do
         for (int j = 0; j < nb; ++j) J[bi[j] * n + si] -= bnu[j] * d;
     }
     const int t = m->rate_type[r];
-    if (t != HC_RATE_ARRHENIUS) {
+    if (t != HC_RATE_ARRHENIUS && t != HC_RATE_PLOG) {   /* hasThirdBodyTerms() */
         double *g = scratch;
         gamDGamDCi(m, r, T, c, g);
         for (int i = 0; i < m->nsp; ++i) {
@@ -487,7 +592,7 @@ static void DqDT(const mech_ctx *x, int r, double kf, double kr, double qfr, dou
     const int nf = m->nf[r], nb = m->nb[r], nsp = m->nsp;
     const int *fi = &m->fidx[HC_MAX_SIDE * r], *bi = &m->bidx[HC_MAX_SIDE * r];
     const double *fnu = &m->fnu[HC_MAX_SIDE * r], *bnu = &m->bnu[HC_MAX_SIDE * r];
-    double dkfdT = rateDkDT(m, r, kf, T, c);
+    double dkfdT = rateDkDT(m, r, kf, x->p, T, c);
     double dkrdT = DkrDT(x, r, kr, T, dkfdT);
     for (int i = 0; i < nf; ++i) dkfdT *= pow(hmax(c[fi[i]], 0.0), m->ford[HC_MAX_SIDE * r + i]);
     for (int i = 0; i < nb; ++i) dkrdT *= pow(hmax(c[bi[i]], 0.0), m->bord[HC_MAX_SIDE * r + i]);
@@ -847,14 +952,14 @@ void oracle_thermo(const hc_mech_desc *m, double T, double *out) {
     }
 }
 
-/* rate constants at (T, c): out[3*nrc] = kf, Kc, kr */
-void oracle_rates(const hc_mech_desc *m, double T, const double *c, double *out) {
-    mech_ctx x = {m, (double *)xcalloc(m->nsp, 8), (double *)xcalloc(m->nsp, 8)};
+/* rate constants at (p, T, c): out[3*nrc] = kf, Kc, kr */
+void oracle_rates(const hc_mech_desc *m, double p, double T, const double *c, double *out) {
+    mech_ctx x = {m, (double *)xcalloc(m->nsp, 8), (double *)xcalloc(m->nsp, 8), p};
     double *cc = (double *)xcalloc(m->nsp, 8);
     for (int i = 0; i < m->nsp; ++i) cc[i] = hmax(c[i], 0.0);
     updateG0(&x, T);
     for (int r = 0; r < m->nrc; ++r) {
-        const double kf = rateK(m, r, T, cc);
+        const double kf = rateK(m, r, p, T, cc);
         out[3 * r] = kf;
         out[3 * r + 1] = Kc(&x, r, T);
         out[3 * r + 2] = kRev(&x, r, kf, T, cc);
@@ -877,9 +982,11 @@ static void reactorFree(reactor *R) {
     free(R->x.G0); free(R->x.DG0DT); free(R->ci); free(R->g);
 }
 
-/* DyDt and Jacobian at states: y = [c, T] per state */
+/* DyDt and Jacobian at states: y = [c, T] per state, at pressures p[ns]
+   (NULL: one atmosphere; only pressure-dependent rate tables read it) */
 void oracle_rhs_jac(const hc_mech_desc *m, int64_t ns, const double *c /*[nsp*ns]*/,
-                    const double *T, double *dydt /*[ns*n]*/, double *J /*[ns*n*n]*/) {
+                    const double *T, const double *p, double *dydt /*[ns*n]*/,
+                    double *J /*[ns*n*n]*/) {
     reactor R;
     reactorInit(&R, m);
     const int n = R.n;
@@ -887,6 +994,7 @@ void oracle_rhs_jac(const hc_mech_desc *m, int64_t ns, const double *c /*[nsp*ns
     for (int64_t k = 0; k < ns; ++k) {
         for (int i = 0; i < m->nsp; ++i) y[i] = c[(int64_t)i * ns + k];
         y[m->nsp] = T[k];
+        R.p = R.x.p = p ? p[k] : PATM;
         if (dydt) DyDt(&R, y, &dydt[k * n]);
         if (J) jacobian(&R, y, f, &J[k * n * n]);
     }
@@ -935,6 +1043,7 @@ int oracle_integrate(const hc_mech_desc *m, const hc_opts *o, int64_t ncells, do
             continue;
         }
         R.p = p[cell];
+        R.x.p = p[cell];
         double leftTime = tstep;
         double sub = hmin(leftTime, hmin(subdt[cell], o->dt_max));
         double Tcur = Ti;

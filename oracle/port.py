@@ -38,6 +38,16 @@ def _arr_rev(t):
     return np.zeros((t.nrc, 3)) if a is None else a
 
 
+def _plog(t):
+    """PLOG tables (ptr [nrc+1], p [n], arr [n, 3]); empty for tables without them.
+    The arrays are never empty, so that their addresses are valid."""
+    ptr = getattr(t, "plog_ptr", None)
+    if ptr is None:
+        return np.zeros(t.nrc + 1, np.int32), np.zeros(1), np.zeros((1, 3))
+    return (ptr, t.plog_p if len(t.plog_p) else np.zeros(1),
+            t.plog_arr if len(t.plog_arr) else np.zeros((1, 3)))
+
+
 class HcMechDesc(C.Structure):
     _fields_ = [
         ("nsp", C.c_int32), ("nrc", C.c_int32),
@@ -48,6 +58,7 @@ class HcMechDesc(C.Structure):
         ("fnu", C.c_void_p), ("bnu", C.c_void_p), ("ford", C.c_void_p), ("bord", C.c_void_p),
         ("geom", C.c_void_p), ("eps_k", C.c_void_p), ("sigma", C.c_void_p),
         ("sri", C.c_void_p), ("arr_rev", C.c_void_p),
+        ("plog_ptr", C.c_void_p), ("plog_p", C.c_void_p), ("plog_arr", C.c_void_p),
     ]
 
 
@@ -90,7 +101,8 @@ class MechDesc:
             arr0=f64(t.arr0), troe=f64(t.troe), eff=f64(t.eff), nf=i32(t.nf), nb=i32(t.nb),
             fidx=i32(t.fidx), bidx=i32(t.bidx), fnu=f64(t.fnu), bnu=f64(t.bnu),
             ford=f64(t.ford), bord=f64(t.bord), geom=i32(t.geom), eps_k=f64(t.eps_k),
-            sigma=f64(t.sigma), sri=f64(_sri(t)), arr_rev=f64(_arr_rev(t)))
+            sigma=f64(t.sigma), sri=f64(_sri(t)), arr_rev=f64(_arr_rev(t)),
+            plog_ptr=i32(_plog(t)[0]), plog_p=f64(_plog(t)[1]), plog_arr=f64(_plog(t)[2]))
         d = HcMechDesc()
         d.nsp, d.nrc = t.nsp, t.nrc
         for k, a in self.arrays.items():
@@ -109,9 +121,10 @@ def lib():
         _lib.oracle_integrate.restype = C.c_int
         _lib.oracle_integrate.argtypes = [C.POINTER(HcMechDesc), C.POINTER(HcOpts), C.c_int64] + \
             [C.c_void_p] * 5 + [C.c_double] + [C.c_void_p] * 4
-        _lib.oracle_rhs_jac.argtypes = [C.POINTER(HcMechDesc), C.c_int64] + [C.c_void_p] * 4
+        _lib.oracle_rhs_jac.argtypes = [C.POINTER(HcMechDesc), C.c_int64] + [C.c_void_p] * 5
         _lib.oracle_thermo.argtypes = [C.POINTER(HcMechDesc), C.c_double, C.c_void_p]
-        _lib.oracle_rates.argtypes = [C.POINTER(HcMechDesc), C.c_double, C.c_void_p, C.c_void_p]
+        _lib.oracle_rates.argtypes = [C.POINTER(HcMechDesc), C.c_double, C.c_double, C.c_void_p,
+                                      C.c_void_p]
     return _lib
 
 
@@ -172,14 +185,19 @@ def integrate(md: MechDesc, T, p, rho, Y, dt, subdt=None, dt_factor=1.0,
             "counters": counters}
 
 
-def rhs_jac(md: MechDesc, c, T):
+def rhs_jac(md: MechDesc, c, T, p=None):
+    """DyDt and the Jacobian at states (c [nsp, ns], T [ns]) and pressures p
+    ([ns] or a scalar; one atmosphere when None -- only pressure-dependent rate
+    tables read it)."""
     c = np.ascontiguousarray(c, dtype=np.float64)
     T = np.ascontiguousarray(T, dtype=np.float64)
     ns = T.shape[0]
     n = md.nsp + 1
     dydt = np.zeros((ns, n))
     J = np.zeros((ns, n, n))
-    lib().oracle_rhs_jac(C.byref(md.desc), ns, _p(c), _p(T), _p(dydt), _p(J))
+    pp = None if p is None else np.ascontiguousarray(np.broadcast_to(np.asarray(p, np.float64), (ns,)))
+    lib().oracle_rhs_jac(C.byref(md.desc), ns, _p(c), _p(T), None if pp is None else _p(pp),
+                         _p(dydt), _p(J))
     return dydt, J
 
 
@@ -189,8 +207,8 @@ def thermo(md: MechDesc, T: float) -> np.ndarray:
     return out
 
 
-def rates(md: MechDesc, T: float, c) -> np.ndarray:
+def rates(md: MechDesc, T: float, c, p: float = 101325.0) -> np.ndarray:
     c = np.ascontiguousarray(c, dtype=np.float64)
     out = np.zeros((md.nrc, 3))
-    lib().oracle_rates(C.byref(md.desc), float(T), _p(c), _p(out))
+    lib().oracle_rates(C.byref(md.desc), float(p), float(T), _p(c), _p(out))
     return out

@@ -26,7 +26,7 @@ def srcimp(t, T, p, rho, Y):
     Y = np.asarray(Y, np.float64)
     nsp = t.nsp
     c = rho[None, :] * Y / t.W[:, None]
-    f, J = port.rhs_jac(port.MechDesc(t), c, T)
+    f, J = port.rhs_jac(port.MechDesc(t), c, T, p)
     Ri = f[:, :nsp].T * t.W[:, None]
     pr = props_oracle.properties(t, T, p, Y)
     R = props_oracle.RU / t.W

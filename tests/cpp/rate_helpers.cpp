@@ -1,0 +1,39 @@
+// Host build of the device rate-law helpers (openhurricane_b200/csrc/rtc_base.cuh)
+// for a CPU check of their arithmetic. Reads from stdin, printing 17
+// significant digits:
+//   "S a b c d e T Pr F DPrDT"  -> sri_F, sri_dfdt, sri_dfdci_factor
+//   "P n p T  p_1 A_1 b_1 Ta_1 ... p_n A_n b_n Ta_n"  -> plog_k, plog_dkdt
+#include <cmath>
+#include <cstdio>
+
+using std::isinf;
+using std::isnan;
+
+#include "../../openhurricane_b200/csrc/rtc_base.cuh"
+
+int main() {
+    char kind[2];
+    while (std::scanf("%1s", kind) == 1) {
+        if (kind[0] == 'S') {
+            double s[5], T, Pr, F, DPrDT;
+            if (std::scanf("%lf %lf %lf %lf %lf %lf %lf %lf %lf", &s[0], &s[1], &s[2], &s[3], &s[4],
+                           &T, &Pr, &F, &DPrDT) != 9)
+                return 1;
+            std::printf("%.17g %.17g %.17g\n", hc::sri_F(s, T, Pr),
+                        hc::sri_dfdt(s, T, Pr, F, DPrDT), hc::sri_dfdci_factor(s, T, Pr, F));
+        } else if (kind[0] == 'P') {
+            int n = 0;
+            double p, T, pp[16], pa[48];
+            if (std::scanf("%d %lf %lf", &n, &p, &T) != 3 || n < 1 || n > 16) return 1;
+            for (int i = 0; i < n; ++i)
+                if (std::scanf("%lf %lf %lf %lf", &pp[i], &pa[3 * i], &pa[3 * i + 1],
+                               &pa[3 * i + 2]) != 4)
+                    return 1;
+            const double k = hc::plog_k(pp, pa, n, p, T, std::log(T));
+            std::printf("%.17g %.17g\n", k, hc::plog_dkdt(pp, pa, n, k, p, T, std::log(T)));
+        } else {
+            return 1;
+        }
+    }
+    return 0;
+}

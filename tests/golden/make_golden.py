@@ -15,8 +15,10 @@ and stores inputs and outputs:
                   dt = 1e-7 s; plus KAT states and properties of 16 cells.
   ext_ref.npz   : 9-species / 21-reaction mechanism with the rate forms beyond
                   the small one (SRI, REV, FORD / RORD, REACTIONS-line and
-                  per-reaction units; synth.extended_mechanism), 24 cells drawn
-                  like the small workload, dt = 1e-6 s; plus KAT states,
+                  per-reaction units, PLOG; synth.extended_mechanism), 48 cells
+                  drawn like the small workload, dt = 1e-7 s (at 1e-6 s some
+                  of its cells answer one-ulp input changes with 1e-6 changes
+                  of T); plus KAT states,
                   point-implicit source terms and properties of 16 cells.
 
 The mechanism files are regenerated from their seeds by
@@ -114,7 +116,7 @@ def main():
              os.path.join(HERE, "large_ref.npz"))
     if "ext" in which:
         ext = synth.extended_mechanism()
-        make("ext", ext, synth.dirichlet_cells(9, 24, seed=109), 1e-6, 8,
+        make("ext", ext, synth.dirichlet_cells(9, 48, seed=109), 1e-7, 8,
              synth.dirichlet_cells(9, 16, seed=111), os.path.join(HERE, "ext_ref.npz"))
 
 

@@ -129,8 +129,10 @@ def _che(body, header="REACTIONS"):
 
 def test_reader_rejects_what_it_does_not_take():
     import pytest
-    with pytest.raises(NotImplementedError, match="PLOG"):
-        M.parse_chemkin(_che("H2+O2=2HO 1.0E13 0.0 1000.0\n PLOG / 1.0 1.0E13 0.0 1000.0 /"))
+    with pytest.raises(NotImplementedError, match="CHEB"):
+        M.parse_chemkin(_che("H2+O2=2HO 1.0E13 0.0 1000.0\n CHEB / 7 4 /"))
+    with pytest.raises(ValueError, match="PLOG"):
+        M.parse_chemkin(_che("H2+O2+M=2HO+M 1.0E13 0.0 1000.0\n PLOG / 1.0 1.0E13 0.0 1000.0 /"))
     with pytest.raises(ValueError, match="FORD"):
         M.parse_chemkin(_che("H2+O2=2HO 1.0E13 0.0 1000.0\n FORD / O 0.5 /"))
     with pytest.raises(ValueError, match="unit"):
@@ -138,3 +140,32 @@ def test_reader_rejects_what_it_does_not_take():
     names, _, rx = M.parse_chemkin(_che(
         "H+O2(+M)=HO+O(+M) 1.0E13 0.0 1000.0\n LOW / 1.0E16 0.0 0.0 /\n REV / 1.0E12 0.0 0.0 /"))
     assert rx[0].rev is not None and rx[0].kind == "falloff"
+
+
+def test_plog_tables_are_sorted_and_converted(ext, tmp_path):
+    """PLOG entries sorted by pressure (equal pressures in file order), in Pa,
+    with the reaction's A and E factors; a repeated highest pressure is
+    refused (the reference's derivative reads past its table there)."""
+    import pytest
+    t = ext["tables"]
+    rows = np.flatnonzero(t.rate_type == M.RATE_PLOG)
+    assert len(rows) == 3 and t.plog_ptr[-1] == 9
+    for r in rows:
+        pp = t.plog_p[t.plog_ptr[r]:t.plog_ptr[r + 1]]
+        assert (np.diff(pp) >= 0).all() and pp[-1] > pp[-2]
+    assert set(np.round(t.plog_p / M.PATM, 6)) == {0.01, 0.1, 0.5, 1.0, 10.0, 100.0}
+    src = [r for r in ext["mech"].reactions if r.plog]
+    dup = [r for r in src if r.plog[0][0] == r.plog[1][0]][0]
+    r = [i for i in rows if t.plog_p[t.plog_ptr[i]] == t.plog_p[t.plog_ptr[i] + 1]][0]
+    b = t.plog_ptr[r]
+    # file order kept for the equal pressures; A in kmol-m-s (order 2: x 1e-3)
+    assert np.allclose(t.plog_arr[b:b + 2, 0], [dup.plog[0][1] * 1e-3, dup.plog[1][1] * 1e-3],
+                       rtol=1e-6)
+    che = _che("H2+O2=2HO 1.0E13 0.0 1000.0\n PLOG / 1.0 1.0E13 0.0 1000.0 /\n"
+               " PLOG / 1.0 2.0E13 0.0 1000.0 /")
+    names, els, rx = M.parse_chemkin(che)
+    assert len(rx[0].plog) == 2
+    f = tmp_path / "m.che"
+    f.write_text(che)
+    with pytest.raises(ValueError, match="highest pressure"):
+        M.compile_mechanism(str(f), *ext["files"][1:])

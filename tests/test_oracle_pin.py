@@ -54,12 +54,13 @@ def test_oracle_kernels_bit_exact_vs_reference_golden(name, request):
     mk = request.getfixturevalue(name)
     g = _load(name)
     md = port.MechDesc(mk["tables"])
-    dydt, J = port.rhs_jac(md, g["kat_c"], g["kat_T"])
+    dydt, J = port.rhs_jac(md, g["kat_c"], g["kat_T"], g["kat_p"])
     assert np.array_equal(dydt, g["kat_dydt"])
     assert np.array_equal(J, g["kat_J"])
     for s in range(g["kat_T"].shape[0]):
         assert np.array_equal(port.thermo(md, g["kat_T"][s]), g["kat_thermo"][s])
-        assert np.array_equal(port.rates(md, g["kat_T"][s], g["kat_c"][:, s]), g["kat_rates"][s])
+        assert np.array_equal(port.rates(md, g["kat_T"][s], g["kat_c"][:, s], g["kat_p"][s]),
+                              g["kat_rates"][s])
 
 
 @pytest.mark.parametrize("name", ["small", "large", "ext"])
