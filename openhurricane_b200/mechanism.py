@@ -36,8 +36,9 @@ parameters); reversible (=, <=>) and irreversible (=>) reactions; explicit
 reverse Arrhenius parameters (REV, reversibleReactionWithRevPars) on
 Arrhenius and third-body reactions; non-stoichiometric orders (FORD, RORD).
 pressure-dependent Arrhenius tables (PLOG, logInterpolationRR) on reactions
-without a third body. The reference's other rate forms (CHEB, HIGH, LT,
-JAN, ...) are rejected with NotImplementedError.
+without a third body. The reference's other rate forms (HIGH, LT, JAN, ...)
+are rejected with NotImplementedError, and so is CHEB, whose reference
+implementation does not evaluate the Chebyshev fit (see parse_chemkin).
 """
 from __future__ import annotations
 
@@ -280,6 +281,19 @@ def parse_chemkin(che_text: str, species_names: Optional[List[str]] = None):
                 raise ValueError(f"unexpected word {word!r} in {line.strip()!r}")
             up = key.upper()
             v = val.split()
+            if up in ("CHEB", "PCHEB", "TCHEB"):
+                # ChebyshevPolynomialsRR (ChebyshevPolynomialsRR.cpp:173-236,
+                # ChebyshevPolynomialsRR.hpp:85-98, 105-114) evaluates
+                # 0.001 log10 of the polynomial sum (the fit is 10 to that
+                # power), keeps the transforms of its default 300-2500 K and
+                # 0.001-100 atm ranges whatever TCHEB / PCHEB say, and divides
+                # its temperature derivative by max(1/Tmax - 1/Tmin, tiny),
+                # which is tiny; restating it would give a rate that is not the
+                # file's fit, so such reactions are refused
+                raise NotImplementedError(
+                    f"{up}: the reference's Chebyshev rate (ChebyshevPolynomialsRR) does not "
+                    "evaluate the Chebyshev fit (0.001*log10 of the sum, default ranges, "
+                    "a 1e-15 divisor in dk/dT); reactions using it are not taken")
             if up in _UNSUPPORTED_AUX:
                 raise NotImplementedError(f"rate form {up} is not supported by this reader")
             if up == "LOW":
