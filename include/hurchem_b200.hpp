@@ -59,6 +59,35 @@ public:
     hc_mech_t handle() const { return h_; }
     void setTuning(int kernel, int block) { check(hc_set_tuning(h_, kernel, block), "hc_set_tuning"); }
 
+    /*
+     * The reference's CUDA-path buffers, one record of nsp + 2 doubles per cell
+     * in host memory. integrateRecords: records [T, Y..., rho] over dt (already
+     * times dtFactor) from the warm-start sub-steps subdt (updated), as
+     * calcChemODEsArray (CUDAChemistrySourceODEs.cu:823-858) leaves them:
+     * T and c_i with the record's rho when returnCi, else T, Y and the new rho.
+     * Returns the number of cells that hit the step-size floor or the Newton cap.
+     * p may be null (ideal-gas pressure from the record).
+     */
+    int integrateRecords(int64_t ncells, double *TYiRho, const double *dt, double *subdt,
+                         bool returnCi, const hc_opts &opts = defaultOptions(),
+                         const double *p = nullptr) {
+        return check(hc_integrate_aos_host(h_, &opts, ncells, TYiRho, p, dt, subdt,
+                                           returnCi ? 1 : 0, nullptr, nullptr),
+                     "hc_integrate_aos_host");
+    }
+    /*
+     * Source terms from records [Y..., rho, T] into RRi[cell * nsp + i], enqueued
+     * on `stream` (a cudaStream_t) without waiting: the caller does its own work
+     * and synchronises the stream before reading RRi (calculateSourceTermsAsync,
+     * CUDAChemistrySource.cpp:189-198). Pinned host buffers make the copies
+     * asynchronous.
+     */
+    void sourceTermsRecordsAsync(int64_t ncells, const double *YiRhoT, double *RRi,
+                                 void *stream, const double *p = nullptr) {
+        check(hc_source_terms_aos_async(h_, ncells, YiRhoT, p, RRi, stream),
+              "hc_source_terms_aos_async");
+    }
+
 private:
     hc_mech_t h_ = nullptr;
 };
