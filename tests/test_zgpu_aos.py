@@ -70,12 +70,12 @@ def test_integrate_records_match_species_major_fields(small, return_ci, given_p)
     dev = _dev()
     t = small["tables"]
     m = Mechanism(t)
-    n = 1500                          # not a multiple of the 32-cell tile
+    n = 301                           # not a multiple of the 32-cell tile
     T, p, rho, Y = _cells(t, n, seed=811)
     if not given_p:
         p = _ideal_gas_p(t.W, T, rho, Y)
-    dt = np.full(n, 1e-6)
-    sub = np.full(n, 1e-6)
+    dt = np.full(n, 1e-7)
+    sub = np.full(n, 1e-7)
     opts = _capi.default_opts(**workloads.SOLVER_OPTS)
     Ts, rs, Ys, ss = _soa_integrate(m, opts, T, p, rho, Y, dt, sub)
 
@@ -104,17 +104,17 @@ def test_integrate_records_host_form_matches_device_form(small):
     dev = _dev()
     t = small["tables"]
     m = Mechanism(t)
-    n = 777
+    n = 77
     T, p, rho, Y = _cells(t, n, seed=812)
     opts = _capi.default_opts(**workloads.SOLVER_OPTS)
     rec0 = _pack_integration(T, Y, rho)
-    dt = np.full(n, 1e-6)
+    dt = np.full(n, 1e-7)
     rec_d = torch.tensor(rec0, device=dev)
-    sub_d = torch.full((n,), 1e-6, dtype=torch.float64, device=dev)
+    sub_d = torch.full((n,), 1e-7, dtype=torch.float64, device=dev)
     m.integrate_aos(rec_d, torch.tensor(dt, device=dev), sub_d, return_ci=True, opts=opts)
     torch.cuda.synchronize()
     rec_h = rec0.copy()
-    sub_h = np.full(n, 1e-6)
+    sub_h = np.full(n, 1e-7)
     st_h = np.zeros(n, np.int32)
     rc = _capi.load().hc_integrate_aos_host(m.handle, C.byref(opts), n,
                                             rec_h.ctypes.data_as(C.c_void_p), None,
