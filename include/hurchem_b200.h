@@ -57,6 +57,8 @@ extern "C" {
 #define HC_RATE_SRI 5       /* fall-off with the SRI function (fallOffFunctions::SRI) */
 #define HC_RATE_PLOG 6      /* pressure-dependent Arrhenius table with logarithmic
                                interpolation, Chemkin PLOG (logInterpolationRR) */
+#define HC_RATE_LANDAU_TELLER 7   /* A T^b exp(-Ta/T + B/T^(1/3) + C/T^(2/3)), Chemkin LT
+                                     (LandauTellerRR) */
 
 /* hc_mech_desc.reversible */
 #define HC_IRREVERSIBLE 0
@@ -108,6 +110,12 @@ typedef struct hc_mech_desc {
     const int32_t *plog_ptr; /* [nrc+1] */
     const double *plog_p;    /* [plog_ptr[nrc]] pressures, Pa */
     const double *plog_arr;  /* [plog_ptr[nrc]*3] A, beta, Ta of each entry */
+    /* chemically activated bimolecular reactions (Chemkin HIGH,
+       chemicallyActicatedBimolecularRR): 1 where the fall-off reaction r
+       (HC_RATE_LINDEMANN / TROE3 / TROE4 / SRI) is one, with arr0 = k0 (its main
+       line) and arr = kinf (HIGH); k = k0 F / (1 + Pr). NULL: none */
+    const int32_t *activated; /* [nrc] */
+    const double *lt;        /* [nrc*2] Landau-Teller B, C (HC_RATE_LANDAU_TELLER); NULL: none */
 } hc_mech_desc;
 
 /*

@@ -36,6 +36,12 @@ def _arr_rev(t):
     return np.zeros((t.nrc, 3)) if a is None else a
 
 
+def _opt(t, name, shape, dtype):
+    """An optional per-reaction table, zeros for tables without it."""
+    a = getattr(t, name, None)
+    return np.zeros(shape, dtype) if a is None else a
+
+
 def _plog(t):
     """PLOG tables (ptr [nrc+1], p [n], arr [n, 3]); empty for tables without them.
     The arrays are never empty, so that their addresses are valid."""
@@ -57,6 +63,7 @@ class HcMechDesc(C.Structure):
         ("geom", C.c_void_p), ("eps_k", C.c_void_p), ("sigma", C.c_void_p),
         ("sri", C.c_void_p), ("arr_rev", C.c_void_p),
         ("plog_ptr", C.c_void_p), ("plog_p", C.c_void_p), ("plog_arr", C.c_void_p),
+        ("activated", C.c_void_p), ("lt", C.c_void_p),
     ]
 
 
@@ -194,7 +201,9 @@ class DescArrays:
             fidx=i32(t.fidx), bidx=i32(t.bidx), fnu=f64(t.fnu), bnu=f64(t.bnu),
             ford=f64(t.ford), bord=f64(t.bord), geom=i32(t.geom), eps_k=f64(t.eps_k),
             sigma=f64(t.sigma), sri=f64(_sri(t)), arr_rev=f64(_arr_rev(t)),
-            plog_ptr=i32(_plog(t)[0]), plog_p=f64(_plog(t)[1]), plog_arr=f64(_plog(t)[2]))
+            plog_ptr=i32(_plog(t)[0]), plog_p=f64(_plog(t)[1]), plog_arr=f64(_plog(t)[2]),
+            activated=i32(_opt(t, "activated", (t.nrc,), np.int32)),
+            lt=f64(_opt(t, "lt", (t.nrc, 2), np.float64)))
         d = HcMechDesc()
         d.nsp, d.nrc = int(t.nsp), int(t.nrc)
         for k, a in self.arrays.items():

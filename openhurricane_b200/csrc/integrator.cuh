@@ -177,7 +177,7 @@ struct CellCtx {
             bo[k] = (k < nb) ? ldg(&m.bord[kMaxSide * r + k]) : 0.0;
         }
         double M = 0.0;
-        if (type != kArrhenius && !(X && type == kPLOG)) {
+        if (type != kArrhenius && !(X && (type == kPLOG || type == kLandauTeller))) {
             const double *e = &m.eff[(int64_t)r * nsp];
             for (int i = 0; i < nsp; ++i) M += ldg(&e[i]) * c[i];
         }
@@ -189,6 +189,8 @@ struct CellCtx {
             kf = M * arrK_log(A, b, Ta, T, logT);
         } else if (X && type == kPLOG) {
             kf = plog_k_global(m.plog_ptr, m.plog_p, m.plog_arr, r, p, T, logT);
+        } else if (X && type == kLandauTeller) {
+            kf = lt_k_global(&m.arr[3 * r], &m.lt[2 * r], T, logT);
         } else {
             const double A0 = ldg(&m.arr0[3 * r]);
             b0 = ldg(&m.arr0[3 * r + 1]);
@@ -202,7 +204,9 @@ struct CellCtx {
                 if (type != kLindemann) lf = troe_logfcent(&m.troe[4 * r], type == kTroe4, T);
                 F = fall_F(type, lf, Pr);
             }
-            kf = kinf * (Pr / (1.0 + Pr)) * F;
+            // chemicallyActicatedBimolecularRR::k (chemicallyActicatedBimolecularRR.cpp:36-44)
+            if (X && ldg(&m.activated[r])) kf = k0 * (1.0 / (1.0 + Pr)) * F;
+            else kf = kinf * (Pr / (1.0 + Pr)) * F;
         }
         double kr = 0.0, Kc = 0.0, DKcDT = 0.0;
         const int rev_kind = ldg(&m.reversible[r]);
@@ -286,6 +290,10 @@ struct CellCtx {
             dkfdT = kf * invT * (b + Ta * invT);
         } else if (X && type == kPLOG) {
             dkfdT = plog_dkdt_global(m.plog_ptr, m.plog_p, m.plog_arr, r, kf, p, T, logT);
+        } else if (X && type == kLandauTeller) {
+            dkfdT = lt_dkdt_global(&m.arr[3 * r], &m.lt[2 * r], kf, T);
+        } else if (X && ldg(&m.activated[r])) {
+            dkfdT = (1.0 / (1.0 + Pr)) * F * (k0 * invT * (b0 + Ta0 * invT));
         } else {
             dkfdT = (Pr / (1.0 + Pr)) * F * (kinf * invT * (b + Ta * invT));
         }
@@ -309,7 +317,7 @@ struct CellCtx {
         if (type == kThirdBody) {
             kind = 1.0;
             rec[11] = q / hmax(M, kTiny);
-        } else if (type != kArrhenius && !(X && type == kPLOG)) {
+        } else if (type != kArrhenius && !(X && (type == kPLOG || type == kLandauTeller))) {
             if (M > kTiny) {
                 // unimolecularFallOffRR::gamDGamDT (unimolecularFallOffRR.cpp:55-91)
                 const double Pr2 = k0 * M / notZeroD(kinf);
@@ -320,12 +328,20 @@ struct CellCtx {
                 const double dFdT = (X && type == kSRI)
                                         ? sri_dfdt_global(&m.sri[5 * r], T, Pr2, F2, dPrdT)
                                         : troe_dfdt(type, &m.troe[4 * r], T, Pr2, F2, dPrdT);
-                dgdT = q * (dPrdT / (Pr2 * (1 + Pr2)) + dFdT / F2);
                 const double fabc = (X && type == kSRI)
                                         ? sri_dfdci_factor_global(&m.sri[5 * r], T, Pr2, F2)
                                         : troe_dfdci_factor(type, lf, Pr2, F2);
-                const double g = q * (k0 / notZeroD(kinf)) *
-                                 (1.0 / (Pr2 * (1 + Pr2)) + fabc * (1.0 / Pr2) / F2);
+                double g;
+                if (X && ldg(&m.activated[r])) {
+                    // chemicallyActicatedBimolecularRR::gamDGamDT / gamDGamDCi
+                    // (chemicallyActicatedBimolecularRR.cpp:56-96)
+                    dgdT = q * (-dPrdT / (1 + Pr2) + dFdT / F2);
+                    g = q * (k0 / notZeroD(kinf)) * (-1.0 / (1 + Pr2) + fabc * (1.0 / Pr2) / F2);
+                } else {
+                    dgdT = q * (dPrdT / (Pr2 * (1 + Pr2)) + dFdT / F2);
+                    g = q * (k0 / notZeroD(kinf)) *
+                        (1.0 / (Pr2 * (1 + Pr2)) + fabc * (1.0 / Pr2) / F2);
+                }
                 kind = finite(g) ? 2.0 : 3.0;
                 rec[11] = g;
             } else {

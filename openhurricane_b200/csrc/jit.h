@@ -19,10 +19,13 @@ struct HostMech {
     std::vector<int32_t> rate_type, reversible, nf, nb, fidx, bidx;
     std::vector<double> arr, arr0, troe, eff, fnu, bnu, ford, bord, sum_stoi;
     std::vector<double> sri, arr_rev;
+    std::vector<int32_t> activated;        // [nrc] chemically activated bimolecular
+    std::vector<double> lt;                // [nrc*2] Landau-Teller B, C
     std::vector<int32_t> plog_ptr;         // [nrc+1], in device reaction order
     std::vector<double> plog_p, plog_arr;
     // the mechanism uses rate forms only the cell-group kernels evaluate
-    // (SRI fall-off, explicit reverse parameters, PLOG tables)
+    // (SRI fall-off, explicit reverse parameters, PLOG tables, chemically
+    // activated and Landau-Teller rates)
     bool ext = false;
 };
 

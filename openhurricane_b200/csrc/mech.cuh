@@ -20,7 +20,9 @@ struct DevMech {
     const int32_t *rate_type, *reversible;
     const double *arr, *arr0, *troe;  // [nrc*3], [nrc*3], [nrc*4]
     const double *sri, *arr_rev;      // [nrc*5] SRI a..e, [nrc*3] explicit reverse Arrhenius
-    int32_t ext;                      // any SRI, REV or PLOG reaction
+    int32_t ext;                      // any SRI, REV, PLOG, HIGH or LT reaction
+    const int32_t *activated;         // [nrc] chemically activated bimolecular (HIGH)
+    const double *lt;                 // [nrc*2] Landau-Teller B, C
     const int32_t *plog_ptr;          // [nrc+1] PLOG entries of each reaction
     const double *plog_p, *plog_arr;  // [n] Pa, [n*3] A, beta, Ta
     const double *eff;      // [nrc*nsp]
@@ -136,6 +138,16 @@ static __device__ __noinline__ double plog_dkdt_global(const int32_t *ptr, const
                                                       double p, double T, double logT) {
     const int b = ldg(&ptr[r]), n = ldg(&ptr[r + 1]) - b;
     return plog_dkdt(&pp[b], &pa[3 * b], n, kj, p, T, logT);
+}
+
+static __device__ __noinline__ double lt_k_global(const double *a, const double *bc, double T,
+                                                 double logT) {
+    return lt_k(ldg(&a[0]), ldg(&a[1]), ldg(&a[2]), ldg(&bc[0]), ldg(&bc[1]), T, logT);
+}
+
+static __device__ __noinline__ double lt_dkdt_global(const double *a, const double *bc, double k,
+                                                    double T) {
+    return lt_dkdt(k, ldg(&a[1]), ldg(&a[2]), ldg(&bc[0]), ldg(&bc[1]), T);
 }
 
 static __device__ __noinline__ double arr_global(const double *a, double T, double logT) {

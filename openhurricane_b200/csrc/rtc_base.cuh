@@ -26,7 +26,8 @@ constexpr double kRu = (1.380649e-23 * 6.02214076e23) * 1e3;
 constexpr int kMaxSide = 4;
 
 enum RateType : int32_t {
-    kArrhenius = 0, kThirdBody = 1, kLindemann = 2, kTroe3 = 3, kTroe4 = 4, kSRI = 5, kPLOG = 6
+    kArrhenius = 0, kThirdBody = 1, kLindemann = 2, kTroe3 = 3, kTroe4 = 4, kSRI = 5, kPLOG = 6,
+    kLandauTeller = 7
 };
 // reversible flags: 1 kr = kf / Kc, 2 kr from explicit reverse Arrhenius parameters
 constexpr int32_t kRevExplicit = 2;
@@ -229,6 +230,28 @@ __device__ __forceinline__ double plog_dkdt(const double *pp, const double *pa, 
     const double lnp0 = log(pp[i]), lnp1 = log(pp[i + 1]), lnp = log(p);
     const double dlnkdT = 1.0 / k0 * dk0 + (1.0 / k1 * dk1 - 1.0 / k0 * dk0) * (lnp - lnp0) / (lnp1 - lnp0);
     return kj * dlnkdT;
+}
+
+// Landau-Teller (LandauTellerRR::k, ::DkDT, LandauTellerRR.cpp:37-99):
+// k = A T^b exp(-Ta/T + B T^(-1/3) + C T^(-2/3)),
+// dk/dT = k (b + Ta/T - B T^(-1/3) / 3 - 2 C T^(-2/3) / 3) / T
+__device__ __forceinline__ double lt_k(double A, double b, double Ta, double B, double C, double T,
+                                       double logT) {
+    double e = 0.0;
+    if (fabs(b) > kVeryTiny) e = b * logT;
+    if (fabs(Ta) > kVeryTiny) e -= Ta / T;
+    if (fabs(B) > kVeryTiny) e += B / cbrt(T);
+    if (fabs(C) > kVeryTiny) e += C / pow(T, 2.0 / 3.0);
+    return A * exp(e);
+}
+
+__device__ __forceinline__ double lt_dkdt(double k, double b, double Ta, double B, double C,
+                                          double T) {
+    double d = 0.0;
+    if (fabs(Ta) > kVeryTiny) d += Ta / T;
+    if (fabs(B) > kVeryTiny) d -= (B / cbrt(T)) / 3.0;
+    if (fabs(C) > kVeryTiny) d -= 2.0 * (C / pow(T, 2.0 / 3.0)) / 3.0;
+    return k * (b + d) / T;
 }
 
 struct IntegratorParams {

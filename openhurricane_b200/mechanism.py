@@ -36,9 +36,12 @@ parameters); reversible (=, <=>) and irreversible (=>) reactions; explicit
 reverse Arrhenius parameters (REV, reversibleReactionWithRevPars) on
 Arrhenius and third-body reactions; non-stoichiometric orders (FORD, RORD).
 pressure-dependent Arrhenius tables (PLOG, logInterpolationRR) on reactions
-without a third body. The reference's other rate forms (HIGH, LT, JAN, ...)
-are rejected with NotImplementedError, and so is CHEB, whose reference
-implementation does not evaluate the Chebyshev fit (see parse_chemkin).
+without a third body; chemically activated bimolecular reactions (HIGH,
+chemicallyActicatedBimolecularRR) with any fall-off function; Landau-Teller
+rates (LT, LandauTellerRR). The reference's other rate forms (RLT, JAN,
+FIT1, ...) are rejected with NotImplementedError, and so is CHEB, whose
+reference implementation does not evaluate the Chebyshev fit (see
+parse_chemkin).
 """
 from __future__ import annotations
 
@@ -75,6 +78,7 @@ RATE_TROE3 = 3
 RATE_TROE4 = 4
 RATE_SRI = 5
 RATE_PLOG = 6
+RATE_LANDAU_TELLER = 7
 
 # reversibility codes
 IRREVERSIBLE = 0
@@ -89,7 +93,7 @@ UNITS_E = {"CAL": "CAL", "CAL/MOLE": "CAL", "EVOL": "EVOL", "EVOLTS": "EVOL", "J
            "KELVINS": "KELV", "KJOU": "KJOU", "KJOULES/MOLE": "KJOU"}
 ELECTRON_VOLT = 1.6021766208e-19    # J (physicalConstant.hpp:59,114)
 # auxiliary keywords of the reference's reader that this reader does not take
-_UNSUPPORTED_AUX = {"CHEB", "PCHEB", "TCHEB", "HIGH", "LT", "RLT", "JAN", "FIT1", "TDEP",
+_UNSUPPORTED_AUX = {"CHEB", "PCHEB", "TCHEB", "RLT", "JAN", "FIT1", "TDEP",
                     "XSMI", "MOME", "EXCI", "COLLEFF"}
 
 
@@ -112,6 +116,8 @@ class ParsedReaction:
     units_A: str = "MOLES"
     units_E: str = "CAL"
     plog: Optional[List[Tuple[float, float, float, float]]] = None   # (p atm, A, b, E) as read
+    high: Optional[Tuple[float, float, float]] = None   # HIGH A, b, E (chemically activated)
+    lt: Optional[Tuple[float, float]] = None             # Landau-Teller B, C
 
 
 @dataclasses.dataclass
@@ -151,6 +157,8 @@ class MechTables:
     plog_ptr: Optional[np.ndarray] = None  # [nrc + 1] int32 entries of each PLOG reaction
     plog_p: Optional[np.ndarray] = None    # [n] Pa, sorted per reaction
     plog_arr: Optional[np.ndarray] = None  # [n, 3] A, beta, Ta
+    activated: Optional[np.ndarray] = None  # [nrc] int32 1: chemically activated (HIGH)
+    lt: Optional[np.ndarray] = None        # [nrc, 2] Landau-Teller B, C
 
     @property
     def nsp(self) -> int:
@@ -313,6 +321,16 @@ def parse_chemkin(che_text: str, species_names: Optional[List[str]] = None):
                 if cur.plog is None:
                     cur.plog = []
                 cur.plog.append(tuple(_read_real(x) for x in v))
+            elif up == "HIGH":
+                # chemkinFileRead.cpp:311-344: a (+M) reaction whose main line is k0
+                if cur.kind != "falloff":
+                    raise ValueError("HIGH needs a pressure-dependent (+M) reaction")
+                cur.high = (_read_real(v[0]), _read_real(v[1]), _read_real(v[2]))
+            elif up == "LT":
+                # chemkinFileRead.cpp:413-440: not on a pressure-dependent reaction
+                if cur.kind != "arrhenius":
+                    raise ValueError("LT cannot be used on a third-body or fall-off reaction")
+                cur.lt = (_read_real(v[0]), _read_real(v[1]))
             elif up == "REV":
                 cur.rev = (_read_real(v[0]), _read_real(v[1]), _read_real(v[2]))
             elif up in ("FORD", "RORD"):
@@ -450,6 +468,8 @@ def compile_mechanism(che_path: str, thermo_path: str, transport_path: str) -> M
     bord = np.zeros((nrc, MAX_SIDE))
     sum_stoi = np.zeros(nrc)
     plog_rows = []
+    activated = np.zeros(nrc, np.int32)
+    lt = np.zeros((nrc, 2))
     for r, rx in enumerate(reactions):
         if len(rx.fwd) > MAX_SIDE or len(rx.bwd) > MAX_SIDE:
             raise ValueError("too many species on one side")
@@ -476,6 +496,13 @@ def compile_mechanism(che_path: str, thermo_path: str, transport_path: str) -> M
             rate_type[r] = RATE_PLOG
             arr[r] = (rx.A * Afac, rx.b, rx.E / Efac)
             plog_rows.append((r, [(pa * PATM, A_ * Afac, b_, E_ / Efac) for pa, A_, b_, E_ in ent]))
+        elif rx.lt is not None:
+            if rx.rev is not None:
+                # the reference needs RLT with REV here, which this reader does not take
+                raise ValueError("REV on a Landau-Teller reaction")
+            rate_type[r] = RATE_LANDAU_TELLER
+            arr[r] = (rx.A * Afac, rx.b, rx.E / Efac)
+            lt[r] = rx.lt
         elif rx.kind == "arrhenius":
             rate_type[r] = RATE_ARRHENIUS
             arr[r] = (rx.A * Afac, rx.b, rx.E / Efac)
@@ -484,13 +511,24 @@ def compile_mechanism(che_path: str, thermo_path: str, transport_path: str) -> M
             arr[r] = (1e-3 * rx.A * Afac, rx.b, rx.E / Efac)
             eff[r] = rx.eff
         else:
-            if rx.low is None:
-                raise ValueError("fall-off reaction without LOW")
             if rx.rev is not None:
                 raise ValueError("REV cannot be used with a fall-off rate (chemkinFileRead.cpp:1460)")
-            A0, b0, E0 = rx.low
-            arr0[r] = (A0 * (1e-3 * Afac), b0, E0 / Efac)
-            arr[r] = (rx.A * Afac, rx.b, rx.E / Efac)
+            if rx.high is not None:
+                # chemicallyActicatedBimolecularRR: k0 from the main line, kinf from
+                # HIGH, with A factors Afactor and Afactor / 1e-3
+                # (chemkinFileRead.cpp:1475-1483)
+                if rx.low is not None:
+                    raise ValueError("LOW and HIGH on one reaction")
+                Ah, bh, Eh = rx.high
+                arr0[r] = (rx.A * Afac, rx.b, rx.E / Efac)
+                arr[r] = (Ah * (Afac / 1e-3), bh, Eh / Efac)
+                activated[r] = 1
+            else:
+                if rx.low is None:
+                    raise ValueError("fall-off reaction without LOW")
+                A0, b0, E0 = rx.low
+                arr0[r] = (A0 * (1e-3 * Afac), b0, E0 / Efac)
+                arr[r] = (rx.A * Afac, rx.b, rx.E / Efac)
             eff[r] = rx.eff
             if rx.sri is not None:
                 rate_type[r] = RATE_SRI
@@ -551,7 +589,8 @@ def compile_mechanism(che_path: str, thermo_path: str, transport_path: str) -> M
     return MechTables(names, W, Ri, Tr, nasa, el_names, E, rate_type, rev, arr, arr0, troe,
                       eff, nf, nb, fidx, bidx, fnu, bnu, ford, bord, sum_stoi,
                       geom, eps, sig, dip, pol, zr, sri=sri, arr_rev=arr_rev,
-                      plog_ptr=plog_ptr, plog_p=plog_p, plog_arr=plog_arr)
+                      plog_ptr=plog_ptr, plog_p=plog_p, plog_arr=plog_arr,
+                      activated=activated, lt=lt)
 
 
 def element_matrix_mass(m: MechTables) -> np.ndarray:

@@ -70,6 +70,8 @@ class Reaction:
     units: Optional[str] = None                        # UNITS /.../ of this reaction
     plog: List[Tuple[float, float, float, float]] = dataclasses.field(default_factory=list)
     #                                                  # PLOG p [atm], A, b, Ea (cal/mol)
+    activated: bool = False     # chemically activated: main line = low, HIGH = (A, b, Ea)
+    lt: Optional[Tuple[float, float]] = None           # Landau-Teller B, C
 
 
 @dataclasses.dataclass
@@ -322,7 +324,8 @@ def extended_mechanism(seed: int = 20241117) -> Mechanism:
     third-body reaction, a forward and a reverse order override (FORD 1.5,
     RORD 1.5), energies written in kJ/mol on the REACTIONS line, and
     per-reaction UNITS (molecules for one reaction, kcal/mol for another),
-    and three PLOG pressure tables.
+    three PLOG pressure tables, a chemically activated (HIGH) reaction and a
+    Landau-Teller (LT) one.
     The rate parameters stay those of the drawn mechanism; the file carries
     them in the declared units. (Orders below one give rates that are not
     Lipschitz at zero concentration; with such an order this mechanism's
@@ -342,6 +345,7 @@ def extended_mechanism(seed: int = 20241117) -> Mechanism:
                    float(np.round(rng.uniform(0.8, 1.2), 4)),
                    float(np.round(rng.uniform(-0.3, 0.3), 4)))
     fall[1].troe = None
+    fall[1].activated = True     # chemically activated bimolecular (HIGH) with the SRI form
     plain = [r for r in m.reactions if r.kind == "plain"]
     tb = [r for r in m.reactions if r.kind == "third_body"]
 
@@ -364,6 +368,8 @@ def extended_mechanism(seed: int = 20241117) -> Mechanism:
         r.plog = [(pa, float(r.A * 10.0 ** rng.uniform(-1.0, 1.0)),
                    float(np.round(r.b + rng.uniform(-0.2, 0.2), 6)),
                    float(np.round(r.Ea + rng.uniform(-2000.0, 2000.0), 4))) for pa in ps]
+    plain[9].lt = (float(np.round(rng.uniform(-20.0, 20.0), 4)),
+                   float(np.round(rng.uniform(-50.0, 50.0), 4)))
     return m
 
 
@@ -443,10 +449,16 @@ def write_chemkin(mech: Mechanism, out_dir: str, stem: str = "mech") -> Tuple[st
         third = r.kind != "plain"
         A = lambda a, o: _pre_exp_in(a, o, third, u_A)
         eq = _reaction_side(r.reactants, r.kind) + "=" + _reaction_side(r.products, r.kind)
-        lines.append(f"{eq}   {A(r.A, fo):.6E}  {r.b:.6f}  {E(r.Ea):.4f}")
-        if r.kind == "troe":
+        if r.activated:
+            A0, b0, E0 = r.low
+            lines.append(f"{eq}   {A(A0, fo):.6E}  {b0:.6f}  {E(E0):.4f}")
+            lines.append(f"   HIGH / {A(r.A, fo):.6E}  {r.b:.6f}  {E(r.Ea):.4f} /")
+        else:
+            lines.append(f"{eq}   {A(r.A, fo):.6E}  {r.b:.6f}  {E(r.Ea):.4f}")
+        if r.kind == "troe" and not r.activated:
             A0, b0, E0 = r.low
             lines.append(f"   LOW / {A(A0, fo):.6E}  {b0:.6f}  {E(E0):.4f} /")
+        if r.kind == "troe":
             if r.sri is not None:
                 lines.append("   SRI / " + "  ".join(f"{x:.6g}" for x in r.sri) + " /")
             else:
@@ -464,6 +476,8 @@ def write_chemkin(mech: Mechanism, out_dir: str, stem: str = "mech") -> Tuple[st
             lines.append(f"   UNITS / {r.units} /")
         for pa, Ap, bp, Ep in r.plog:
             lines.append(f"   PLOG / {pa:g}  {A(Ap, fo):.6E}  {bp:.6f}  {E(Ep):.4f} /")
+        if r.lt is not None:
+            lines.append(f"   LT / {r.lt[0]:g}  {r.lt[1]:g} /")
     lines += ["END", ""]
     with open(che, "w") as f:
         f.write("\n".join(lines))

@@ -13,7 +13,9 @@
  *   rate laws     reactionRateTypes/src/ArrheniusRR.cpp:37-47 (+ hpp:96-99),
  *                 ArrheniusThirdBodyRR.cpp:37-57, unimolecularFallOffRR.cpp:37-91,
  *                 fallOffFunctions.cpp:81-157 (Troe), :54-79 (SRI), fallOffFunctions.hpp
- *                 (Lindemann); reversibleReactionWithRevPars.hpp:68-122 (Chemkin REV)
+ *                 (Lindemann); reversibleReactionWithRevPars.hpp:68-122 (Chemkin REV);
+ *                 logInterpolationRR.cpp:78-226 (PLOG), LandauTellerRR.cpp:37-99 (LT),
+ *                 chemicallyActicatedBimolecularRR.cpp:36-96 (HIGH)
  *   reactions     reactionTypes/src/reactionTypes.cpp:178-352 (Kp, DKpDT, Kc, DKcDT, q),
  *                 :354-445 (DqDci), :843-876 (DqDT); reversibleReactions.hpp:62-127;
  *                 irreversibleReactions.hpp; reactionList.hpp:83-86 (updateG0)
@@ -362,11 +364,53 @@ static double plogDkDT(const hc_mech_desc *m, int r, double kj, double p, double
     return dkdT;
 }
 
+/* Landau-Teller (LandauTellerRR.cpp:37-99) */
+static double ltK(const hc_mech_desc *m, int r, double T) {
+    const double *a = &m->arr[3 * r], *bc = &m->lt[2 * r];
+    double lta = a[0];
+    if (fabs(a[1]) > VERY_TINY) lta *= pow(T, a[1]);
+    double expAgr = 0.0;
+    if (fabs(a[2]) > VERY_TINY) expAgr -= a[2] / T;
+    if (fabs(bc[0]) > VERY_TINY) expAgr += bc[0] / pow(T, 1.0 / 3.0);
+    if (fabs(bc[1]) > VERY_TINY) expAgr += bc[1] / pow(T, 2.0 / 3.0);
+    if (fabs(expAgr) > VERY_TINY) lta *= exp(expAgr);
+    return lta;
+}
+
+static double ltDkDT(const hc_mech_desc *m, int r, double T) {
+    const double *a = &m->arr[3 * r], *bc = &m->lt[2 * r];
+    double lta = a[0];
+    if (fabs(a[1]) > VERY_TINY) lta *= pow(T, a[1]);
+    double expArg = 0, deriv = 0;
+    if (fabs(a[2]) > VERY_TINY) {
+        const double TaT = a[2] / T;
+        expArg -= TaT;
+        deriv += TaT;
+    }
+    if (fabs(bc[0]) > VERY_TINY) {
+        const double BT = bc[0] / cbrt(T);
+        expArg += BT;
+        deriv -= BT / 3;
+    }
+    if (fabs(bc[1]) > VERY_TINY) {
+        const double CT = bc[1] / pow(T, 2.0 / 3.0);
+        expArg += CT;
+        deriv -= 2 * CT / 3;
+    }
+    if (fabs(expArg) > VERY_TINY) lta *= exp(expArg);
+    return lta * (a[1] + deriv) / T;
+}
+
+/* chemically activated bimolecular (Chemkin HIGH,
+   chemicallyActicatedBimolecularRR.cpp:36-96): k = k0 F / (1 + Pr) */
+static int activated(const hc_mech_desc *m, int r) { return m->activated && m->activated[r]; }
+
 static double rateK(const hc_mech_desc *m, int r, double p, double T, const double *c) {
     const int t = m->rate_type[r];
     const double *a = &m->arr[3 * r];
     if (t == HC_RATE_ARRHENIUS) return arrK(a, T);
     if (t == HC_RATE_PLOG) return plogK(m, r, p, T);
+    if (t == HC_RATE_LANDAU_TELLER) return ltK(m, r, T);
     if (t == HC_RATE_THIRD_BODY) {
         const double M = thirdM(m, r, c);
         return (M * arrK(a, T));
@@ -374,6 +418,7 @@ static double rateK(const hc_mech_desc *m, int r, double p, double T, const doub
     const double k0 = arrK(&m->arr0[3 * r], T);
     const double kinf = arrK(a, T);
     const double Pr = k0 / notZeroD(kinf) * thirdM(m, r, c);
+    if (activated(m, r)) return k0 * (1.0 / (1.0 + Pr)) * fallF(m, r, T, Pr);
     return kinf * (Pr / (1.0 + Pr)) * fallF(m, r, T, Pr);
 }
 
@@ -383,9 +428,12 @@ static double rateDkDT(const hc_mech_desc *m, int r, double kj, double p, double
     const double *a = &m->arr[3 * r];
     if (t == HC_RATE_ARRHENIUS || t == HC_RATE_THIRD_BODY) return arrDkDT(a, kj, T);
     if (t == HC_RATE_PLOG) return plogDkDT(m, r, kj, p, T);
+    if (t == HC_RATE_LANDAU_TELLER) return ltDkDT(m, r, T);
     const double k0 = arrK(&m->arr0[3 * r], T);
     const double kinf = arrK(a, T);
     const double Pr = k0 / notZeroD(kinf) * thirdM(m, r, c);
+    if (activated(m, r))
+        return (1.0 / (1.0 + Pr)) * fallF(m, r, T, Pr) * arrDkDT(&m->arr0[3 * r], k0, T);
     return (Pr / (1.0 + Pr)) * fallF(m, r, T, Pr) * arrDkDT(a, kinf, T);
 }
 
@@ -407,7 +455,8 @@ static void gamDGamDCi(const hc_mech_desc *m, int r, double T, const double *c, 
         for (int i = 0; i < nsp; ++i) {
             const double dPrdci = e[i] * k0 / notZeroD(kinf);
             const double dFdci = fallDFDci(m, r, T, Pr, F, dPrdci);
-            g[i] = (dPrdci / (Pr * (1 + Pr)) + dFdci / F);
+            if (activated(m, r)) g[i] = (-dPrdci / (1 + Pr) + dFdci / F);
+            else g[i] = (dPrdci / (Pr * (1 + Pr)) + dFdci / F);
         }
     } else {
         for (int i = 0; i < nsp; ++i) g[i] = 0.0;
@@ -416,7 +465,9 @@ static void gamDGamDCi(const hc_mech_desc *m, int r, double T, const double *c, 
 
 static double gamDGamDT(const hc_mech_desc *m, int r, double T, const double *c) {
     const int t = m->rate_type[r];
-    if (t == HC_RATE_ARRHENIUS || t == HC_RATE_THIRD_BODY || t == HC_RATE_PLOG) return 0.0;
+    if (t == HC_RATE_ARRHENIUS || t == HC_RATE_THIRD_BODY || t == HC_RATE_PLOG ||
+        t == HC_RATE_LANDAU_TELLER)
+        return 0.0;
     const double M = thirdM(m, r, c);
     if (M > TINY) {
         const double *a0 = &m->arr0[3 * r], *a = &m->arr[3 * r];
@@ -427,6 +478,7 @@ static double gamDGamDT(const hc_mech_desc *m, int r, double T, const double *c)
         const double dPrdT =
             Pr * (arrDkDT(a0, k0, T) / notZeroD(k0) - arrDkDT(a, kinf, T) / notZeroD(kinf));
         const double dFdT = fallDFDT(m, r, T, Pr, F, dPrdT);
+        if (activated(m, r)) return (-dPrdT / (1 + Pr) + dFdT / F);
         return (dPrdT / (Pr * (1 + Pr)) + dFdT / F);
     }
     return 0.0;
@@ -574,7 +626,8 @@ static void DqDci(const mech_ctx *x, int r, double kf, double kr, double qfr, do
         for (int j = 0; j < nb; ++j) J[bi[j] * n + si] -= bnu[j] * d;
     }
     const int t = m->rate_type[r];
-    if (t != HC_RATE_ARRHENIUS && t != HC_RATE_PLOG) {   /* hasThirdBodyTerms() */
+    if (t != HC_RATE_ARRHENIUS && t != HC_RATE_PLOG &&
+        t != HC_RATE_LANDAU_TELLER) {   /* hasThirdBodyTerms() */
         double *g = scratch;
         gamDGamDCi(m, r, T, c, g);
         for (int i = 0; i < m->nsp; ++i) {

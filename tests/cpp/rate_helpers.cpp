@@ -3,6 +3,7 @@
 // significant digits:
 //   "S a b c d e T Pr F DPrDT"  -> sri_F, sri_dfdt, sri_dfdci_factor
 //   "P n p T  p_1 A_1 b_1 Ta_1 ... p_n A_n b_n Ta_n"  -> plog_k, plog_dkdt
+//   "L A b Ta B C T"  -> lt_k, lt_dkdt
 #include <cmath>
 #include <cstdio>
 
@@ -31,6 +32,11 @@ int main() {
                     return 1;
             const double k = hc::plog_k(pp, pa, n, p, T, std::log(T));
             std::printf("%.17g %.17g\n", k, hc::plog_dkdt(pp, pa, n, k, p, T, std::log(T)));
+        } else if (kind[0] == 'L') {
+            double A, b, Ta, B, C, T;
+            if (std::scanf("%lf %lf %lf %lf %lf %lf", &A, &b, &Ta, &B, &C, &T) != 6) return 1;
+            const double k = hc::lt_k(A, b, Ta, B, C, T, std::log(T));
+            std::printf("%.17g %.17g\n", k, hc::lt_dkdt(k, b, Ta, B, C, T));
         } else {
             return 1;
         }

@@ -98,6 +98,15 @@ def test_extended_rate_forms_are_read(ext):
     assert len(rev) == 3
     assert set(t.rate_type[rev]) == {M.RATE_ARRHENIUS, M.RATE_THIRD_BODY}
     assert (t.arr_rev[rev, 0] > 0).all() and (t.arr_rev[t.reversible != 2] == 0).all()
+    # one chemically activated reaction (HIGH, here with the 5-parameter SRI form):
+    # k0 from its main line (A factor 1e-3 for order 2), kinf from HIGH (x 1e3)
+    act = np.flatnonzero(t.activated)
+    assert len(act) == 1 and t.rate_type[act[0]] == M.RATE_SRI
+    hi = [r for r in m.reactions if r.activated][0]
+    assert np.isclose(t.arr0[act[0], 0], hi.low[0] * 1e-3, rtol=1e-6)
+    assert np.isclose(t.arr[act[0], 0], hi.A * 1e-3 / 1e-3, rtol=1e-6)
+    ltr = np.flatnonzero(t.rate_type == M.RATE_LANDAU_TELLER)
+    assert len(ltr) == 1 and tuple(t.lt[ltr[0]]) == [r for r in m.reactions if r.lt][0].lt
     # the FORD / RORD overrides change the order only, not the stoichiometry
     assert (t.ford != t.fnu).sum() == 1 and t.ford[t.ford != t.fnu][0] == 1.5
     assert (t.bord != t.bnu).sum() == 1 and t.bord[t.bord != t.bnu][0] == 1.5

@@ -5,7 +5,8 @@ SRI::F, SRI::DFDci, SRI::DFDT; the device path folds 1/Pr * dPr/dci out of
 DFDci, as it forms the rank-one third-body column once per reaction, and the
 check multiplies it back in) and the PLOG table (logInterpolationRR.cpp:78-147
 k, :149-226 DkDT, restated loop for loop; the device form evaluates only the
-interval the reference's loop ends on)."""
+interval the reference's loop ends on) and the Landau-Teller rate
+(LandauTellerRR.cpp:37-99)."""
 import math
 import os
 import shutil
@@ -173,3 +174,49 @@ def test_plog_oracle_matches_the_reference_loops(ext):
                 k, _ = _plog_ref([float(x) for x in t.plog_p[b:e]],
                                  [tuple(float(v) for v in a) for a in t.plog_arr[b:e]], p, T)
                 assert kf[r] == k
+
+
+def _lt_ref(A, b, Ta, B, C, T):
+    """LandauTellerRR::k and ::DkDT as written."""
+    lta = A
+    if abs(b) > 1e-300:
+        lta *= math.pow(T, b)
+    e = 0.0
+    if abs(Ta) > 1e-300:
+        e -= Ta / T
+    if abs(B) > 1e-300:
+        e += B / math.pow(T, 1.0 / 3.0)
+    if abs(C) > 1e-300:
+        e += C / math.pow(T, 2.0 / 3.0)
+    k = lta * math.exp(e) if abs(e) > 1e-300 else lta
+    lta = A * (math.pow(T, b) if abs(b) > 1e-300 else 1.0)
+    ea, d = 0.0, 0.0
+    if abs(Ta) > 1e-300:
+        ea -= Ta / T
+        d += Ta / T
+    if abs(B) > 1e-300:
+        bt = B / np.cbrt(T)
+        ea += bt
+        d -= bt / 3
+    if abs(C) > 1e-300:
+        ct = C / math.pow(T, 2.0 / 3.0)
+        ea += ct
+        d -= 2 * ct / 3
+    if abs(ea) > 1e-300:
+        lta *= math.exp(ea)
+    return k, lta * (b + d) / T
+
+
+def test_landau_teller_helpers_match_the_reference(exe):
+    rng = np.random.default_rng(9)
+    cases = [(float(10.0 ** rng.uniform(6, 14)), float(rng.uniform(-1, 2)),
+              float(rng.uniform(0, 3e4)), float(rng.uniform(-40, 40)), float(rng.uniform(-90, 90)),
+              float(rng.uniform(300, 3000))) for _ in range(200)]
+    cases.append((1e10, 0.0, 0.0, 0.0, 0.0, 1000.0))
+    txt = "".join("L " + " ".join(repr(v) for v in c) + "\n" for c in cases)
+    out = subprocess.run([exe], input=txt, capture_output=True, text=True, check=True).stdout
+    got = np.array([[float(x) for x in l.split()] for l in out.strip().splitlines()])
+    for c, g in zip(cases, got):
+        k, d = _lt_ref(*c)
+        assert abs(g[0] - k) <= 1e-13 * abs(k), c
+        assert abs(g[1] - d) <= 1e-12 * max(abs(d), 1e-300) + 1e-14 * abs(k) / c[-1], c
