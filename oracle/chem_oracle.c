@@ -665,13 +665,59 @@ typedef struct {
     double p;
     double *ci, *g, *J, *s;     /* work */
     hc_counters cnt;
+    int cv;                     /* constant volume (else constant pressure) */
+    double rho0;                /* the cell's density (constant volume) */
+    double *yt;                 /* [nsp] mass fractions of the current state */
 } reactor;
+
+/* speciesList::MWbyYi / Rm (speciesList.cpp:106-116, speciesList.inl:58-61) */
+static double mwByYi(const hc_mech_desc *m, const double *yi) {
+    if (m->nsp == 1) return m->W[0];
+    double w = 0.0;
+    for (int i = 0; i < m->nsp; ++i) w += yi[i] / m->W[i];
+    return 1.0 / hmax(w, VERY_TINY);
+}
+
+/* constant volume: p = rho Rm T (perfectGas::pm, perfectGas.cpp:49-53) with
+   Y = c W / rho0 (chemistrySource.cpp:885-906 uses c as given, :975-981 the
+   clamped c), molar internal energy e_i W_i = (h_i - R_i T) W_i
+   (thermo.inl:168-171) and cv_i = cp_i - R_i (thermo.inl:80-94) */
+static double cvPressure(reactor *R, const double *c, double T) {
+    const hc_mech_desc *m = R->x.m;
+    for (int i = 0; i < R->nsp; ++i) R->yt[i] = c[i] * m->W[i] / R->rho0;
+    const double Rm = RU / mwByYi(m, R->yt);
+    return R->rho0 * Rm * T;
+}
+
+static inline double ea_m(const hc_mech_desc *m, int i, double T) {
+    return ha0(m, i, T) - (RU / m->W[i]) * T;
+}
+
+static inline double Cv_p(const hc_mech_desc *m, int i, double T) {
+    return (cp0(m, i, T) - RU / m->W[i]) * m->W[i];
+}
 
 static void DyDt(reactor *R, const double *y, double *dydt) {
     const hc_mech_desc *m = R->x.m;
     const int nsp = R->nsp;
     const double T = y[nsp];
     R->cnt.n_rhs++;
+    if (R->cv) {
+        /* chemistrySource::DyDt, constant volume (chemistrySource.cpp:885-906) */
+        for (int i = 0; i < R->n; ++i) dydt[i] = 0.0;
+        R->p = R->x.p = cvPressure(R, y, T);
+        for (int i = 0; i < nsp; ++i) R->ci[i] = y[i];
+        updateG0(&R->x, T);
+        for (int r = 0; r < m->nrc; ++r) qRate(&R->x, r, T, R->ci, dydt, NULL, NULL);
+        double cvmix = 0.0, DTdt = 0.0;
+        for (int i = 0; i < nsp; ++i) {
+            cvmix += R->yt[i] * (cp0(m, i, T) - RU / m->W[i]);   /* cv_p */
+            DTdt += dydt[i] * ea_m(m, i, T) * m->W[i];
+        }
+        DTdt /= (cvmix * R->rho0);
+        dydt[nsp] = -DTdt;
+        return;
+    }
     for (int i = 0; i < R->n; ++i) dydt[i] = 0.0;
     for (int i = 0; i < nsp; ++i) R->ci[i] = hmax(y[i], 0.0);
     updateG0(&R->x, T);
@@ -693,6 +739,7 @@ static void jacobian(reactor *R, const double *y, double *dfdt, double *J) {
     R->cnt.n_jac++;
     updateG0(&R->x, T);
     for (int i = 0; i < nsp; ++i) R->ci[i] = hmax(y[i], 0.0);
+    if (R->cv) R->p = R->x.p = cvPressure(R, R->ci, T);
     for (int i = 0; i < n * n; ++i) J[i] = 0.0;
     for (int i = 0; i < n; ++i) dfdt[i] = 0.0;
     for (int r = 0; r < m->nrc; ++r) {
@@ -700,6 +747,31 @@ static void jacobian(reactor *R, const double *y, double *dfdt, double *J) {
         const double qfr = qRate(&R->x, r, T, R->ci, dfdt, &kf, &kr);
         DqDci(&R->x, r, kf, kr, qfr, T, R->ci, J, n, R->g);
         DqDT(&R->x, r, kf, kr, qfr, T, R->ci, J, n);
+    }
+    if (R->cv) {
+        /* chemistrySource::jacobian, constant volume (chemistrySource.cpp:1022-1055) */
+        double cCv = 0.0, DTdt = 0.0, dcCvdT = 0.0;
+        for (int i = 0; i < nsp; ++i) {
+            cCv += y[i] * Cv_p(m, i, T);
+            dcCvdT += y[i] * DCp_pDT(m, i, T);
+            DTdt += dfdt[i] * ea_m(m, i, T) * m->W[i];
+        }
+        DTdt /= cCv;
+        dfdt[nsp] = -DTdt;
+        for (int i = 0; i < nsp; ++i) {
+            double d = J[nsp * n + i];
+            for (int j = 0; j < nsp; ++j) d -= J[j * n + i] * ea_m(m, j, T) * m->W[j];
+            d += Cv_p(m, i, T) * DTdt;
+            d /= cCv;
+            J[nsp * n + i] = d;
+        }
+        double dd = 0.0;
+        for (int i = 0; i < nsp; ++i)
+            dd -= (Cv_p(m, i, T) * dfdt[i] + ea_m(m, i, T) * m->W[i] * J[i * n + nsp]);
+        dd += dcCvdT * DTdt;
+        dd /= cCv;
+        J[nsp * n + nsp] = dd;
+        return;
     }
     double cCp = 0.0, DTdt = 0.0, dcCpdT = 0.0;
     for (int i = 0; i < nsp; ++i) {
@@ -1029,10 +1101,11 @@ static void reactorInit(reactor *R, const hc_mech_desc *m) {
     R->n = m->nsp + 1;
     R->ci = (double *)xcalloc(m->nsp, 8);
     R->g = (double *)xcalloc(m->nsp, 8);
+    R->yt = (double *)xcalloc(m->nsp, 8);
 }
 
 static void reactorFree(reactor *R) {
-    free(R->x.G0); free(R->x.DG0DT); free(R->ci); free(R->g);
+    free(R->x.G0); free(R->x.DG0DT); free(R->ci); free(R->g); free(R->yt);
 }
 
 /* DyDt and Jacobian at states: y = [c, T] per state, at pressures p[ns]
@@ -1097,6 +1170,8 @@ int oracle_integrate(const hc_mech_desc *m, const hc_opts *o, int64_t ncells, do
         }
         R.p = p[cell];
         R.x.p = p[cell];
+        R.cv = o->reactor == 1;
+        R.rho0 = rho[cell];
         double leftTime = tstep;
         double sub = hmin(leftTime, hmin(subdt[cell], o->dt_max));
         double Tcur = Ti;
@@ -1123,13 +1198,15 @@ int oracle_integrate(const hc_mech_desc *m, const hc_opts *o, int64_t ncells, do
         }
         if (ys != 1.0)
             for (int i = 0; i < nsp; ++i) yi[i] /= ys;
-        /* rho = p / (Rm T), Rm = Ru / Wmean, Wmean = 1/max(sum yi/Wi, veryTiny)
-           (perfectGas.cpp:36-40, speciesList.inl:58-61, speciesList.cpp:106-116) */
+        /* constant pressure: rho = p / (Rm T), Rm = Ru / Wmean, Wmean =
+           1/max(sum yi/Wi, veryTiny) (perfectGas.cpp:36-40, speciesList.inl:58-61,
+           speciesList.cpp:106-116); constant volume: rho is kept and the reference
+           updates p instead (chemistrySource.cpp:1317-1323) */
         double wsum = 0.0;
         for (int i = 0; i < nsp; ++i) wsum += yi[i] / m->W[i];
         const double Rm = RU / (1.0 / hmax(wsum, VERY_TINY));
         T[cell] = Tcur;
-        rho[cell] = p[cell] / (Rm * Tcur);
+        if (!R.cv) rho[cell] = p[cell] / (Rm * Tcur);
         for (int i = 0; i < nsp; ++i) {
             Y[(int64_t)i * ncells + cell] = yi[i];
             cout[(int64_t)i * ncells + cell] = y[i];

@@ -13,6 +13,10 @@ and stores inputs and outputs:
   large_ref.npz : 53-species / 325-reaction mechanism, 2 cells drawn like the
                   large workload (T 800-2800 K, p 0.5-10 atm, Dirichlet(0.3)),
                   dt = 1e-7 s; plus KAT states and properties of 16 cells.
+  cv_ref.npz    : the constant-volume reactor (chemSolvers type constVolume) on
+                  24 cells of the small mechanism (dt = 1e-6 s) and 24 of the
+                  extended one (dt = 1e-7 s): integrated T, Y, c, sub-steps and
+                  the reference's updated pressure.
   ext_ref.npz   : 9-species / 21-reaction mechanism with the rate forms beyond
                   the small one (SRI, REV, FORD / RORD, REACTIONS-line and
                   per-reaction units, PLOG; synth.extended_mechanism), 48 cells
@@ -25,7 +29,7 @@ The mechanism files are regenerated from their seeds by
 openhurricane_b200.synth at test time; a SHA-256 of the generated text files
 is stored so that a change of the generator is detected.
 
-    python tests/golden/make_golden.py [small] [large] [ext]   (default: all;
+    python tests/golden/make_golden.py [small] [large] [ext] [cv]   (default: all;
     needs oracle/_ref/hurchem_ref)
 """
 import hashlib
@@ -99,10 +103,32 @@ def make(name, mech, cells, dt, nkat, prop_cells, out):
     print(name, "written", out, "reference seconds", res["seconds"])
 
 
+def make_cv(out):
+    """Constant-volume integrations of the small and extended mechanisms."""
+    res = {}
+    for name, mech, dt, seed in (("small", synth.small_mechanism(), 1e-6, 113),
+                                 ("ext", synth.extended_mechanism(), 1e-7, 115)):
+        work = tempfile.mkdtemp(prefix="golden_cv_")
+        files = synth.write_chemkin(mech, work)
+        case = os.path.join(work, "case.cont")
+        refrun.write_case(case, *files, {"atol": 1e-15, "reactor": "constVolume"})
+        cells = synth.dirichlet_cells(len(mech.species), 24, seed=seed)
+        rho = synth.mixture_density(mech.weights(), cells)
+        r = refrun.integrate(case, cells.T, cells.p, rho, dt, dt, cells.Y, procs=os.cpu_count() or 1,
+                             workdir=work)
+        res.update({f"{name}_sha": files_sha(files), f"{name}_dt": dt, f"{name}_in_T": cells.T,
+                    f"{name}_in_p": cells.p, f"{name}_in_rho": rho, f"{name}_in_Y": cells.Y,
+                    f"{name}_out_T": r["T"], f"{name}_out_Y": r["Y"], f"{name}_out_c": r["c"],
+                    f"{name}_out_subdt": r["subdt"], f"{name}_out_p": r["p"],
+                    f"{name}_out_rho": r["rho"]})
+    np.savez_compressed(out, **res)
+    print("cv written", out)
+
+
 def main():
     if not refrun.available():
         raise SystemExit("oracle/_ref/hurchem_ref is missing: make -f oracle/Makefile.ref")
-    which = set(sys.argv[1:]) or {"small", "large", "ext"}
+    which = set(sys.argv[1:]) or {"small", "large", "ext", "cv"}
     if "small" in which:
         small = synth.small_mechanism()
         make("small", small, synth.dirichlet_cells(9, 48, seed=101), 1e-6, 8,
@@ -118,6 +144,8 @@ def main():
         ext = synth.extended_mechanism()
         make("ext", ext, synth.dirichlet_cells(9, 48, seed=109), 1e-7, 8,
              synth.dirichlet_cells(9, 16, seed=111), os.path.join(HERE, "ext_ref.npz"))
+    if "cv" in which:
+        make_cv(os.path.join(HERE, "cv_ref.npz"))
 
 
 if __name__ == "__main__":

@@ -119,3 +119,24 @@ def test_temperature_from_enthalpy_oracle_vs_reference_golden(name, request):
     assert np.array_equal(flag, g["tha_flag"])
     assert np.abs(T - g["tha_T"]).max() < 1e-9
     assert flag[0] == 1   # started at 20 K, below TLow: clamped, then converged inside
+
+
+@pytest.mark.parametrize("name", ["small", "ext"])
+def test_constant_volume_oracle_vs_reference_golden(name, request):
+    """chemistrySource with chemSolvers type constVolume: density held, the
+    temperature equation on internal energy and cv, the pressure following
+    the state (chemistrySource.cpp:885-906, 1022-1055, 1317-1323)."""
+    from oracle import port
+    mk = request.getfixturevalue(name)
+    g = np.load(os.path.join(HERE, "golden", "cv_ref.npz"))
+    assert _sha(mk["files"]) == str(g[f"{name}_sha"])
+    t = mk["tables"]
+    o = port.integrate(port.MechDesc(t), g[f"{name}_in_T"], g[f"{name}_in_p"],
+                       g[f"{name}_in_rho"], g[f"{name}_in_Y"], float(g[f"{name}_dt"]),
+                       opts=port.default_opts(atol=1e-15, reactor=1))
+    for k in ("T", "Y", "c", "subdt", "rho"):
+        assert np.array_equal(o[k], g[f"{name}_out_" + k]), k
+    assert np.array_equal(o["rho"], g[f"{name}_in_rho"])
+    from openhurricane_b200 import mechanism
+    mw = 1.0 / np.maximum((o["Y"] / t.W[:, None]).sum(axis=0), 1e-300)
+    assert np.array_equal(o["rho"] * (mechanism.RU / mw) * o["T"], g[f"{name}_out_p"])
