@@ -131,7 +131,10 @@ typedef struct hc_opts {
     int32_t maxstep;             /* 10000 */
     int32_t auto_update_jacobian;/* 0 */
     int32_t step_to_update_jac;  /* 10 */
-    int32_t reactor;             /* 0 constant pressure (only form built) */
+    int32_t reactor;             /* chemSolvers type: 0 constant pressure, 1 constant volume
+                                    (cell-group kernels: the density is held and not written,
+                                    the pressure follows the state inside the step and is not
+                                    written back, as in the reference's solveUpdate) */
     double atol;                 /* 1e-15 (reference default "tiny") */
     double rtol;                 /* 1e-4 */
     double safescale;            /* 0.8 */

@@ -137,13 +137,14 @@ IntegratorParams make_params(const hc_opts *o) {
     // evaluated with the host libm, as the reference does at run time (ImplicitEuler.cpp:287)
     P.err_accept_limit = std::pow(o->maxscale / o->safescale, -1.0 / o->alphainc);
     P.max_newton_total = o->max_newton_total;
+    P.reactor = o->reactor;
     return P;
 }
 
 int check_opts(const hc_opts *o) {
     if (!o) return fail(HC_E_INVALID, "opts is null");
-    if (o->reactor != 0)
-        return fail(HC_E_UNSUPPORTED, "only the constant-pressure reactor is built");
+    if (o->reactor != 0 && o->reactor != 1)
+        return fail(HC_E_INVALID, "reactor must be 0 (constant pressure) or 1 (constant volume)");
     if (o->maxstep <= 0 || o->step_to_update_jac <= 0)
         return fail(HC_E_INVALID, "maxstep and step_to_update_jac must be positive");
     if (!(o->alphainc > 0) || !(o->safescale > 0))
@@ -592,15 +593,17 @@ static int integrate_impl(hc_mech_t m, const hc_opts *opts, int64_t ncells, doub
     io.queue_head = m->queue;
     io.counters = m->queue + 1;
     const int N = m->dm.nsp + 1;
-    const bool t1_ok = N <= 16 && !opts->auto_update_jacobian && !m->host.ext;
+    const bool t1_ok = N <= 16 && !opts->auto_update_jacobian && !m->host.ext && opts->reactor == 0;
     if (m->kernel == 1 && !t1_ok)
         return fail(HC_E_UNSUPPORTED,
-                    "thread-per-cell kernel needs nsp <= 15, autoUpdateJacobian off and no SRI "
-                    "or explicit reverse (REV), PLOG, HIGH or LT rate laws");
+                    "thread-per-cell kernel needs nsp <= 15, autoUpdateJacobian off, the "
+                    "constant-pressure reactor and no SRI or explicit reverse (REV), PLOG, HIGH or "
+                    "LT rate laws");
     if (m->kernel == 4 && !(t1_ok && m->t2_ok))
         return fail(HC_E_UNSUPPORTED,
                     "compact thread-per-cell kernel needs nsp <= 15, <= 64 reactions, "
-                    "autoUpdateJacobian off and no SRI, explicit reverse (REV), PLOG, HIGH or LT rate laws");
+                    "autoUpdateJacobian off, the constant-pressure reactor and no SRI, explicit "
+                    "reverse (REV), PLOG, HIGH or LT rate laws");
     // automatic choice: the cell group. Per-cell costs in a flow step differ
     // by orders of magnitude, and the step lasts as long as its stiffest
     // cell; the cell group's lanes share each Newton iteration's work and
@@ -623,8 +626,9 @@ static int integrate_impl(hc_mech_t m, const hc_opts *opts, int64_t ncells, doub
     }
     if (m->kernel == 3 && !t1_ok)
         return fail(HC_E_UNSUPPORTED,
-                    "generated thread-per-cell kernel needs nsp <= 15, autoUpdateJacobian off and "
-                    "no SRI, explicit reverse (REV), PLOG, HIGH or LT rate laws");
+                    "generated thread-per-cell kernel needs nsp <= 15, autoUpdateJacobian off, the "
+                    "constant-pressure reactor and no SRI, explicit reverse (REV), PLOG, HIGH or LT "
+                    "rate laws");
     bool use_jit = t1_ok && m->kernel == 3;
     if (use_jit && !m->jit_tried) {
         // first use: generate, compile and load (host work, no stream operation)
@@ -1189,10 +1193,11 @@ extern "C" int hc_integrate_noalloc(hc_mech_t m, const hc_opts *opts, int64_t nc
     if (!T || !p || !rho || !Y || !dt || !subdt) return fail(HC_E_INVALID, "null field");
     if (!(dt_factor > 0)) return fail(HC_E_INVALID, "dt_factor must be positive");
     const int N = m->dm.nsp + 1;
-    if (N > 16 || opts->auto_update_jacobian || !m->t2_ok)
+    if (N > 16 || opts->auto_update_jacobian || !m->t2_ok || opts->reactor != 0)
         return fail(HC_E_UNSUPPORTED,
-                    "hc_integrate_noalloc needs nsp <= 15, <= 64 reactions, autoUpdateJacobian off "
-                    "and no SRI, explicit reverse (REV), PLOG, HIGH or LT rate laws");
+                    "hc_integrate_noalloc needs nsp <= 15, <= 64 reactions, autoUpdateJacobian off, "
+                    "the constant-pressure reactor and no SRI, explicit reverse (REV), PLOG, HIGH or "
+                    "LT rate laws");
     int dev = -1;
     HC_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 256) return fail(HC_E_CUDA, "device ordinal out of range");

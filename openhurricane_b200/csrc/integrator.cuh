@@ -76,32 +76,49 @@ struct CellCtx {
     double *s;        // this cell's shared memory
     int nsp;
     double p;
+    double rho0;      // the cell's density (constant-volume reactor)
     int n_jac, n_rhs, n_lu, n_newton, n_steps, n_attempts;
     int status;
 
     __device__ CellCtx(const DevMech &mm, const IntegratorParams &pp, Group<G> gg, double *sm)
-        : m(mm), P(pp), g(gg), s(sm), nsp(mm.nsp), p(0), n_jac(0), n_rhs(0), n_lu(0),
+        : m(mm), P(pp), g(gg), s(sm), nsp(mm.nsp), p(0), rho0(0), n_jac(0), n_rhs(0), n_lu(0),
           n_newton(0), n_steps(0), n_attempts(0), status(0) {}
 
     // ---------------------------------------------------------------------
     // f(y) and, if jac, the analytic Jacobian rows into shared memory.
     // y is this lane's element (lane < N). Returns this lane's f element.
-    // chemistrySource::DyDt (chemistrySource.cpp:863-883) / ::jacobian (:967-1021)
+    // chemistrySource::DyDt (chemistrySource.cpp:863-883) / ::jacobian (:967-1021);
+    // constant volume (X and P.reactor == 1): :885-906 / :975-981, 1022-1055
     __device__ __forceinline__ double evaluate(double y, bool jac) {
         using L = Smem<N, G>;
         const int lane = g.lane;
+        const bool cv = X && P.reactor == 1;
         if (jac) ++n_jac; else ++n_rhs;
-        if (lane < nsp) s[L::kC + lane] = hmax(y, 0.0);
+        // the constant-volume right-hand side takes c as given, the Jacobian and the
+        // constant-pressure forms the clamped c
+        if (lane < nsp) s[L::kC + lane] = (cv && !jac) ? y : hmax(y, 0.0);
         if (lane == nsp) s[L::kMisc] = y;
         g.sync();
         const double T = s[L::kMisc];
         const double logT = log(T);
+        if (cv) {
+            // p = rho0 Rm T with Y = c W / rho0 (perfectGas::pm, speciesList::MWbyYi)
+            double t = 0.0;
+            if (lane < nsp) {
+                const double Wl = ldg(&m.W[lane]);
+                t = (s[L::kC + lane] * Wl / rho0) / Wl;
+            }
+            const double wsum = g.sum(t);
+            p = rho0 * (kRu / (1.0 / hmax(wsum, kVeryTiny))) * T;
+        }
         if (lane < nsp) {
             const SpeciesThermo th = species_thermo(m, lane, T, logT);
             s[L::kG0 + lane] = th.G0;
             s[L::kDG0 + lane] = th.DG0DT;
-            s[L::kCp + lane] = th.cp;
-            s[L::kH + lane] = th.h;
+            // constant volume: molar Cv = Cp - Ru and E = H - Ru T take the place of
+            // Cp and H in the temperature equation (thermo.inl:80-94, 168-171)
+            s[L::kCp + lane] = cv ? th.cp - kRu : th.cp;
+            s[L::kH + lane] = cv ? th.h - kRu * T : th.h;
             s[L::kDCp + lane] = th.dcp;
         }
         double *Jrow = &s[L::kJ + lane * L::LD];
@@ -132,7 +149,7 @@ struct CellCtx {
             }
             g.sync();
         }
-        // temperature equation (constant pressure)
+        // temperature equation: constant pressure (cp, h) or constant volume (cv, e)
         const bool sp = lane < nsp;
         const double cpi = sp ? s[L::kCp + lane] : 0.0;
         const double hi = sp ? s[L::kH + lane] : 0.0;
@@ -740,6 +757,7 @@ integrate_kernel(const __grid_constant__ DevMech m, const __grid_constant__ Inte
             continue;
         }
         ci.p = io.p[cell];
+        ci.rho0 = io.rho[cell];
         double leftTime = tstep;
         double sub = hmin(leftTime, hmin(io.subdt[cell], P.dt_max));
         if (lane == nsp) y = Ti;
@@ -767,7 +785,9 @@ integrate_kernel(const __grid_constant__ DevMech m, const __grid_constant__ Inte
         }
         if (lane == 0) {
             io.T[cell] = Tn;
-            io.rho[cell] = ci.p / (Rm * Tn);
+            // constant volume keeps the density (the reference updates p instead,
+            // chemistrySource.cpp:1317-1323)
+            if (!(X && P.reactor == 1)) io.rho[cell] = ci.p / (Rm * Tn);
             io.subdt[cell] = sub;
             if (io.status) io.status[cell] = ci.status;
             if (io.cost) io.cost[cell] = ci.n_newton;

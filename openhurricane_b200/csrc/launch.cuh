@@ -27,8 +27,10 @@ struct Launch {
 
     static int integrate(const DevMech &m, int num_sms, const IntegratorParams &P,
                          const CellIO &io, cudaStream_t st, std::string &err) {
-        // the instantiation without the rarer rate forms unless the mechanism has them
-        auto kern = m.ext ? integrate_kernel<N, G, true> : integrate_kernel<N, G, false>;
+        // the instantiation without the rarer rate forms and the constant-volume
+        // reactor unless the mechanism or the options need them
+        auto kern = (m.ext || P.reactor == 1) ? integrate_kernel<N, G, true>
+                                              : integrate_kernel<N, G, false>;
         const size_t sm = smem_bytes();
         HC_LCUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         int per_sm = 0;

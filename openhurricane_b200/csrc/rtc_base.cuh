@@ -262,6 +262,7 @@ struct IntegratorParams {
     double atol_inc, rtol_inc, T_threshold, T_alpha, T_beta, dt_max;
     double err_accept_limit;     // pow(maxscale/safescale, -1/alphainc)
     int64_t max_newton_total;
+    int32_t reactor;             // 0 constant pressure, 1 constant volume (cell group only)
 };
 
 struct CellIO {

@@ -14,9 +14,10 @@ and stores inputs and outputs:
                   large workload (T 800-2800 K, p 0.5-10 atm, Dirichlet(0.3)),
                   dt = 1e-7 s; plus KAT states and properties of 16 cells.
   cv_ref.npz    : the constant-volume reactor (chemSolvers type constVolume) on
-                  24 cells of the small mechanism (dt = 1e-6 s) and 24 of the
-                  extended one (dt = 1e-7 s): integrated T, Y, c, sub-steps and
-                  the reference's updated pressure.
+                  48 cells of the small mechanism (dt = 1e-7 s) and 48 of the
+                  extended one (dt = 3e-8 s; heat release at constant volume
+                  makes longer steps of these cells far stiffer): integrated T,
+                  Y, c, sub-steps and the reference's updated pressure.
   ext_ref.npz   : 9-species / 21-reaction mechanism with the rate forms beyond
                   the small one (SRI, REV, FORD / RORD, REACTIONS-line and
                   per-reaction units, PLOG; synth.extended_mechanism), 48 cells
@@ -106,13 +107,13 @@ def make(name, mech, cells, dt, nkat, prop_cells, out):
 def make_cv(out):
     """Constant-volume integrations of the small and extended mechanisms."""
     res = {}
-    for name, mech, dt, seed in (("small", synth.small_mechanism(), 1e-6, 113),
-                                 ("ext", synth.extended_mechanism(), 1e-7, 115)):
+    for name, mech, dt, seed in (("small", synth.small_mechanism(), 1e-7, 113),
+                                 ("ext", synth.extended_mechanism(), 3e-8, 115)):
         work = tempfile.mkdtemp(prefix="golden_cv_")
         files = synth.write_chemkin(mech, work)
         case = os.path.join(work, "case.cont")
         refrun.write_case(case, *files, {"atol": 1e-15, "reactor": "constVolume"})
-        cells = synth.dirichlet_cells(len(mech.species), 24, seed=seed)
+        cells = synth.dirichlet_cells(len(mech.species), 48, seed=seed)
         rho = synth.mixture_density(mech.weights(), cells)
         r = refrun.integrate(case, cells.T, cells.p, rho, dt, dt, cells.Y, procs=os.cpu_count() or 1,
                              workdir=work)

@@ -149,6 +149,60 @@ def test_extended_rate_forms_parity_vs_oracle(ext, kernel):
     assert (np.abs(g["Ri"] - Ri_o) / scale).max() < 1e-5
 
 
+@pytest.mark.parametrize("name,seed,dt", [("small", 17, 1e-7), ("ext", 19, 3e-8)])
+@pytest.mark.parametrize("kernel", [0, 2])
+def test_constant_volume_reactor_parity_vs_oracle(name, seed, dt, kernel, request):
+    """chemSolvers type constVolume: density held, the temperature equation on
+    internal energy and cv, p following the state (for PLOG rates), through
+    the cell-group kernel, against the oracle (pinned to the reference). The
+    step lengths keep these cells well conditioned (one-ulp input changes move
+    T by at most 2e-11 in the oracle) and cheap (at most 44515 Newton
+    iterations a cell); the cap bounds a cell that would take another path."""
+    mk = request.getfixturevalue(name)
+    t = mk["tables"]
+    T, p, rho, Y = _cells(t, 96, seed=seed)
+    m = _mech(t)
+    m.set_tuning(kernel, 64)
+    g = _gpu_integrate(m, T, p, rho, Y, dt, reactor=1, max_newton_total=1000000, **PARITY)
+    o = _oracle(t, T, p, rho, Y, dt, key=f"cv-{name}", reactor=1, **PARITY)
+    assert np.array_equal(g["status"] & 12, np.zeros_like(g["status"]))
+    _assert_close(g, o, f"constant volume {name}, kernel {kernel}")
+    assert np.array_equal(g["rho"], rho)
+    assert (g["T"] > T).any()
+
+
+@pytest.mark.parametrize("name", ["small", "ext"])
+def test_constant_volume_reactor_vs_reference_golden(name, request):
+    """The reference's own constant-volume outputs at its default rtol:
+    statistical agreement as for the constant-pressure golden cases."""
+    import os
+    mk = request.getfixturevalue(name)
+    here = os.path.dirname(os.path.abspath(__file__))
+    g0 = np.load(os.path.join(here, "golden", "cv_ref.npz"))
+    m = _mech(mk["tables"])
+    g = _gpu_integrate(m, g0[name + "_in_T"], g0[name + "_in_p"], g0[name + "_in_rho"],
+                       g0[name + "_in_Y"], float(g0[name + "_dt"]), atol=1e-15, reactor=1,
+                       max_newton_total=1000000)
+    ref_T, ref_Y = g0[name + "_out_T"], g0[name + "_out_Y"]
+    dT = np.abs(g["T"] - ref_T) / ref_T
+    assert dT.max() < 1e-4
+    dY = np.abs(g["Y"] - ref_Y) - Y_RTOL * np.abs(ref_Y) - Y_FLOOR
+    ok = (dT <= T_RTOL) & (dY.max(axis=0) <= 0.0)
+    assert ok.mean() >= 0.9, f"{ok.mean():.3f} of cells within parity tolerance"
+    assert np.array_equal(g["rho"], g0[name + "_in_rho"])
+
+
+@pytest.mark.parametrize("kernel", [1, 3, 4])
+def test_constant_volume_refused_by_thread_per_cell_kernels(small, kernel):
+    from openhurricane_b200 import _capi
+    t = small["tables"]
+    T, p, rho, Y = _cells(t, 8, seed=18)
+    m = _mech(t)
+    m.set_tuning(kernel, 64)
+    with pytest.raises(_capi.HcError, match="constant-pressure"):
+        _gpu_integrate(m, T, p, rho, Y, 1e-7, reactor=1, **PARITY)
+
+
 @pytest.mark.parametrize("kernel", [1, 3, 4])
 def test_extended_rate_forms_refused_by_thread_per_cell_kernels(ext, kernel):
     from openhurricane_b200 import _capi
