@@ -303,6 +303,17 @@ int hc_temperature_from_enthalpy(hc_mech_t mech, int64_t n, const double *ha, co
                                  int32_t *flag, void *stream);
 
 /*
+ * Temperature from the mixture's mass internal energy at constant density
+ * (thermoList::TEa_rho, thermoList.inl:343-348, the same Newton iteration,
+ * tolerance, cap and clamp as hc_temperature_from_enthalpy):
+ * ea[n] J/kg with e = sum_i Y_i h_i - p/rho, p = rho Rm T; Y[nsp*n], rho[n],
+ * starting temperatures T0[n] -> T[n]; flag[n] (optional) as above.
+ */
+int hc_temperature_from_energy(hc_mech_t mech, int64_t n, const double *ea, const double *Y,
+                               const double *rho, const double *T0, double TLow, double THigh,
+                               double *T, int32_t *flag, void *stream);
+
+/*
  * Point-implicit source terms for the flow solver's species equations
  * (chemistrySource::calculateSourceTermsImp with its default
  * withoutLastSpec = true, chemistrySource.cpp:1412-1450, via omegaCoupled,

@@ -122,6 +122,8 @@ SIGNATURES = {
     "hc_source_terms_imp": (C.c_int, [_VP, C.c_int64] + [_VP] * 6 + [_VP]),
     "hc_temperature_from_enthalpy": (C.c_int, [_VP, C.c_int64] + [_VP] * 3 +
                                      [C.c_double, C.c_double] + [_VP] * 3),
+    "hc_temperature_from_energy": (C.c_int, [_VP, C.c_int64] + [_VP] * 4 +
+                                   [C.c_double, C.c_double] + [_VP] * 3),
     "hc_source_terms_host": (C.c_int, [_VP, C.c_int64] + [_VP] * 5 + [_VP]),
     "hc_properties_host": (C.c_int, [_VP, C.c_int64] + [_VP] * 8 + [_VP]),
     "hc_integrate_aos": (C.c_int, [_VP, C.POINTER(HcOpts), C.c_int64] + [_VP] * 4 +

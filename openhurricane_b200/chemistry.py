@@ -150,6 +150,20 @@ class Mechanism:
         _capi.check(rc, "hc_temperature_from_enthalpy")
         return T, flag
 
+    def temperature_from_energy(self, ea, Y, rho, T0, TLow: float = 50.0, THigh: float = 5000.0,
+                                stream=None):
+        """T from the mixture's mass internal energy at constant density
+        (thermoList::TEa_rho); returns (T, flag)."""
+        n = ea.shape[0]
+        T = torch.empty_like(_f64(ea, "ea"))
+        flag = torch.empty(n, dtype=torch.int32, device=ea.device)
+        rc = _capi.load().hc_temperature_from_energy(self.handle, n, _ptr(ea), _ptr(_f64(Y, "Y")),
+                                                     _ptr(_f64(rho, "rho")), _ptr(_f64(T0, "T0")),
+                                                     float(TLow), float(THigh), _ptr(T),
+                                                     _ptr(flag), _stream(stream))
+        _capi.check(rc, "hc_temperature_from_energy")
+        return T, flag
+
     def properties(self, T, p, Y, stream=None) -> Dict[str, torch.Tensor]:
         """ha [nsp,n] J/kg, cp [n] J/kg/K, mu [n] Pa s, kappa [n] W/m/K, D [nsp,n] m^2/s."""
         n = T.shape[0]

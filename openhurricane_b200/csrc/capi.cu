@@ -818,6 +818,17 @@ int hc_temperature_from_enthalpy(hc_mech_t m, int64_t n, const double *ha, const
                             static_cast<cudaStream_t>(stream), g_err);
 }
 
+int hc_temperature_from_energy(hc_mech_t m, int64_t n, const double *ea, const double *Y,
+                               const double *rho, const double *T0, double TLow, double THigh,
+                               double *T, int32_t *flag, void *stream) {
+    if (!m) return fail(HC_E_INVALID, "null mechanism");
+    if (n <= 0) return HC_OK;
+    if (!ea || !Y || !rho || !T0 || !T) return fail(HC_E_INVALID, "null field");
+    if (!(TLow > 0) || !(THigh > TLow)) return fail(HC_E_INVALID, "need 0 < TLow < THigh");
+    return launch_t_from_ea(m->dm, n, ea, Y, rho, T0, TLow, THigh, T, flag,
+                            static_cast<cudaStream_t>(stream), g_err);
+}
+
 int hc_properties(hc_mech_t m, int64_t n, const double *T, const double *p, const double *Y,
                   double *ha, double *cp, double *mu, double *kappa, double *D, void *stream) {
     if (!m) return fail(HC_E_INVALID, "null mechanism");

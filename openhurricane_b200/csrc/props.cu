@@ -194,6 +194,71 @@ __global__ void t_from_ha_kernel(const __grid_constant__ DevMech m, int64_t n,
     }
 }
 
+// thermoList::TEa_rho (thermoList.inl:343-348 through thermoList.cpp:501-533):
+// the same Newton iteration on the mixture's internal energy at fixed
+// density, e(T) = sum_i Y_i h_i(T) - p / rho with p = rho Rm T, and
+// de/dT = sum_i Y_i cp_i(T) - Rm (thermoList.inl:145-162, 302-306)
+__global__ void t_from_ea_kernel(const __grid_constant__ DevMech m, int64_t n,
+                                 const double *__restrict__ ea, const double *__restrict__ Y,
+                                 const double *__restrict__ rho, const double *__restrict__ T0,
+                                 double TLow, double THigh, double tol, int max_iter,
+                                 double *__restrict__ Tout, int32_t *__restrict__ flag) {
+    const int nsp = m.nsp;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        double w = 0.0;
+        for (int i = 0; i < nsp; ++i) w += Y[(int64_t)i * n + c] / ldg(&m.W[i]);
+        const double Rm = kRu / (1.0 / hmax(w, kVeryTiny));
+        const double r = rho[c];
+        double Tnew = T0[c];
+        const double Ttol = T0[c] * tol;
+        int it = 0, f = 1;
+        while (true) {
+            const double Test = Tnew;
+            double hm = 0.0, cpm = 0.0;
+            for (int i = 0; i < nsp; ++i) {
+                double cp, h;
+                species_cp_h(m, i, Test, cp, h);
+                const double yi = Y[(int64_t)i * n + c];
+                hm += h * yi;
+                cpm += cp * yi;
+            }
+            const double em = hm - (r * Rm * Test) / r;
+            const double cvm = cpm - Rm;
+            const double v = Test - (em - ea[c]) / cvm;
+            if (v < TLow) {
+                f = 0;
+                Tnew = TLow;
+            } else if (v > THigh) {
+                f = 2;
+                Tnew = THigh;
+            } else {
+                f = 1;
+                Tnew = v;
+            }
+            if (it++ > max_iter) break;
+            if (!(fabs(Tnew - Test) > Ttol)) break;
+        }
+        Tout[c] = Tnew;
+        if (flag) flag[c] = f;
+    }
+}
+
+int launch_t_from_ea(const DevMech &m, int64_t n, const double *ea, const double *Y,
+                     const double *rho, const double *T0, double TLow, double THigh, double *T,
+                     int32_t *flag, cudaStream_t st, std::string &err) {
+    if (n <= 0) return HC_OK;
+    const int64_t blocks = (n + 127) / 128;
+    t_from_ea_kernel<<<(unsigned)(blocks < 148 * 64 ? blocks : 148 * 64), 128, 0, st>>>(
+        m, n, ea, Y, rho, T0, TLow, THigh, 1.0e-4, 100, T, flag);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        err = std::string("t_from_ea_kernel: ") + cudaGetErrorString(e);
+        return HC_E_CUDA;
+    }
+    return HC_OK;
+}
+
 int launch_t_from_ha(const DevMech &m, int64_t n, const double *ha, const double *Y,
                      const double *T0, double TLow, double THigh, double *T, int32_t *flag,
                      cudaStream_t st, std::string &err) {

@@ -50,6 +50,9 @@ namespace hc {
 int launch_t_from_ha(const DevMech &m, int64_t n, const double *ha, const double *Y,
                      const double *T0, double TLow, double THigh, double *T, int32_t *flag,
                      cudaStream_t st, std::string &err);
+int launch_t_from_ea(const DevMech &m, int64_t n, const double *ea, const double *Y,
+                     const double *rho, const double *T0, double TLow, double THigh, double *T,
+                     int32_t *flag, cudaStream_t st, std::string &err);
 }
 
 namespace hc {

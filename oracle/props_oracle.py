@@ -114,3 +114,58 @@ def temperature_from_ha(t, ha, p, Y, T0, TLow=50.0, THigh=5000.0, tol=1e-4, max_
         Tout[k] = Tnew
         flag[k] = f
     return Tout, flag
+
+
+def temperature_from_ea(t, ea, rho, Y, T0, TLow=50.0, THigh=5000.0, tol=1e-4, max_iter=100):
+    """thermoList::TEa_rho (thermoList.inl:343-348 through thermoList.cpp:501-533):
+    the same Newton iteration as THa_p on the mixture's internal energy at
+    fixed density, e(T) = sum_i Y_i h_i(T) - p / rho with p = rho Rm T
+    (thermoList.inl:302-306, perfectGas.cpp:49-53) and de/dT = cv =
+    sum_i Y_i cp_i(T) - Rm (thermoList.inl:145-162)."""
+    ea = np.asarray(ea, float)
+    rho = np.asarray(rho, float)
+    Y = np.asarray(Y, float)
+    T0 = np.asarray(T0, float)
+    n = ea.shape[0]
+    Tout = np.empty(n)
+    flag = np.empty(n, np.int32)
+    for k in range(n):
+        w = 0.0
+        for i in range(t.nsp):
+            w += Y[i, k] / t.W[i]
+        Rm = RU / (1.0 / max(w, 1e-300))
+        Tnew = T0[k]
+        Ttol = T0[k] * tol
+        it = 0
+        f = 1
+        while True:
+            Test = Tnew
+            cp, h = species_cp_h(t, np.array([Test]))
+            em = float((h[:, 0] * Y[:, k]).sum()) - (rho[k] * Rm * Test) / rho[k]
+            cvm = float((cp[:, 0] * Y[:, k]).sum()) - Rm
+            v = Test - (em - ea[k]) / cvm
+            if v < TLow:
+                f, Tnew = 0, TLow
+            elif v > THigh:
+                f, Tnew = 2, THigh
+            else:
+                f, Tnew = 1, v
+            it += 1
+            if it - 1 > max_iter:
+                break
+            if not (abs(Tnew - Test) > Ttol):
+                break
+        Tout[k] = Tnew
+        flag[k] = f
+    return Tout, flag
+
+
+def mixture_ea(t, T, rho, Y):
+    """The mixture's internal energy e = sum_i Y_i h_i - rho Rm T / rho [J/kg]."""
+    T = np.asarray(T, float)
+    rho = np.asarray(rho, float)
+    Y = np.asarray(Y, float)
+    cp, h = species_cp_h(t, T)
+    w = (Y / t.W[:, None]).sum(axis=0)
+    Rm = RU / (1.0 / np.maximum(w, 1e-300))
+    return (h * Y).sum(axis=0) - (rho * Rm * T) / rho

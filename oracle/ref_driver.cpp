@@ -306,6 +306,31 @@ static int runSrcImp(OracleChem &chem) {
     return 0;
 }
 
+// thermoList::TEa_rho for each cell: the cells format carries rho, the
+// mixture's internal energy in the dt column and T0 in the sub-step column
+static int runTEa(flowModel &flows) {
+    std::ifstream fin(envOr("HC_IN", "cells.bin"), std::ios::binary);
+    int64_t hdr[2];
+    fin.read(reinterpret_cast<char *>(hdr), sizeof(hdr));
+    const int64_t nsp = hdr[0], n = hdr[1];
+    auto T = readDoubles(fin, n), p = readDoubles(fin, n), rho = readDoubles(fin, n);
+    auto ea = readDoubles(fin, n), T0 = readDoubles(fin, n), Y = readDoubles(fin, nsp * n);
+    const auto &thl = flows.mixtures().thermalTable();
+    std::ofstream fout(envOr("HC_OUT", "tea.bin"), std::ios::binary);
+    int64_t oh[1] = {n};
+    fout.write(reinterpret_cast<const char *>(oh), sizeof(oh));
+    realArray yi(nsp);
+    std::vector<double> out;
+    for (int64_t k = 0; k < n; ++k) {
+        for (int64_t i = 0; i < nsp; ++i) yi[i] = Y[i * n + k];
+        integer flag = 1;
+        out.push_back(thl.TEa_rho(ea[k], rho[k], T0[k], flag, yi));
+        out.push_back((double)flag);
+    }
+    writeDoubles(fout, out);
+    return 0;
+}
+
 static void onSegv(int) {
     void *bt[64];
     int n = backtrace(bt, 64);
@@ -345,6 +370,7 @@ int main(int argc, char *argv[]) {
     else if (mode == "props") rc = runProps(*flows);
     else if (mode == "srcimp") rc = runSrcImp(chem);
     else if (mode == "tha") rc = runTHa(*flows);
+    else if (mode == "tea") rc = runTEa(*flows);
     else rc = 3;
     std::fflush(stdout);
     std::fflush(stderr);

@@ -247,3 +247,19 @@ def tha(case: str, ha, p, T0, Y, workdir: Optional[str] = None) -> Dict[str, np.
     _run(case, {"HC_MODE": "tha", "HC_IN": cells, "HC_OUT": out}, tmp)
     d = np.fromfile(out, dtype=np.float64, offset=8).reshape(n, 2)
     return {"T": d[:, 0].copy(), "iflag": d[:, 1].astype(np.int32)}
+
+
+def tea(case: str, ea, rho, T0, Y, workdir: Optional[str] = None) -> Dict[str, np.ndarray]:
+    """The reference's temperature from mixture internal energy at constant
+    density (thermoList::TEa_rho) for each cell, starting from T0; returns T
+    and iFlag."""
+    tmp = workdir or tempfile.mkdtemp(prefix="hctea_")
+    Y = np.ascontiguousarray(Y, dtype=np.float64)
+    nsp, n = Y.shape
+    cells = os.path.join(tmp, "cells_tea.bin")
+    # the cells format carries ea in the dt column and T0 in the subDt0 column
+    write_cells(cells, np.asarray(T0, np.float64), np.full(n, 101325.0), rho, ea, T0, Y)
+    out = os.path.join(tmp, "tea.bin")
+    _run(case, {"HC_MODE": "tea", "HC_IN": cells, "HC_OUT": out}, tmp)
+    d = np.fromfile(out, dtype=np.float64, offset=8).reshape(n, 2)
+    return {"T": d[:, 0].copy(), "iflag": d[:, 1].astype(np.int32)}

@@ -17,7 +17,9 @@ and stores inputs and outputs:
                   48 cells of the small mechanism (dt = 1e-7 s) and 48 of the
                   extended one (dt = 3e-8 s; heat release at constant volume
                   makes longer steps of these cells far stiffer): integrated T,
-                  Y, c, sub-steps and the reference's updated pressure.
+                  Y, c, sub-steps and the reference's updated pressure; and
+                  thermoList::TEa_rho (temperature from internal energy at
+                  constant density) on 16 cells of each.
   ext_ref.npz   : 9-species / 21-reaction mechanism with the rate forms beyond
                   the small one (SRI, REV, FORD / RORD, REACTIONS-line and
                   per-reaction units, PLOG; synth.extended_mechanism), 48 cells
@@ -45,7 +47,8 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from openhurricane_b200 import synth  # noqa: E402
-from oracle import refrun  # noqa: E402
+from openhurricane_b200.mechanism import compile_mechanism  # noqa: E402
+from oracle import props_oracle, refrun  # noqa: E402
 
 
 def files_sha(paths):
@@ -122,6 +125,17 @@ def make_cv(out):
                     f"{name}_out_T": r["T"], f"{name}_out_Y": r["Y"], f"{name}_out_c": r["c"],
                     f"{name}_out_subdt": r["subdt"], f"{name}_out_p": r["p"],
                     f"{name}_out_rho": r["rho"]})
+        # temperature from internal energy at constant density (thermoList::TEa_rho):
+        # 16 cells' own energy, started 300 K away (and once from 20 K)
+        tc = synth.dirichlet_cells(len(mech.species), 16, seed=seed + 1)
+        trho = synth.mixture_density(mech.weights(), tc)
+        tables = compile_mechanism(*files)
+        ea = props_oracle.mixture_ea(tables, tc.T, trho, tc.Y)
+        T0 = tc.T + np.where(np.arange(16) % 2 == 0, 300.0, -300.0)
+        T0[0] = 20.0
+        te = refrun.tea(case, ea, trho, T0, tc.Y, workdir=work)
+        res.update({f"{name}_tea_ea": ea, f"{name}_tea_rho": trho, f"{name}_tea_Y": tc.Y,
+                    f"{name}_tea_T0": T0, f"{name}_tea_T": te["T"], f"{name}_tea_flag": te["iflag"]})
     np.savez_compressed(out, **res)
     print("cv written", out)
 

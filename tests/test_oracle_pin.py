@@ -140,3 +140,17 @@ def test_constant_volume_oracle_vs_reference_golden(name, request):
     from openhurricane_b200 import mechanism
     mw = 1.0 / np.maximum((o["Y"] / t.W[:, None]).sum(axis=0), 1e-300)
     assert np.array_equal(o["rho"] * (mechanism.RU / mw) * o["T"], g[f"{name}_out_p"])
+
+
+@pytest.mark.parametrize("name", ["small", "ext"])
+def test_temperature_from_energy_oracle_vs_reference_golden(name, request):
+    """thermoList::TEa_rho: Newton on the mixture's internal energy at fixed
+    density with the reference's tolerance, cap and clamp."""
+    from oracle import props_oracle
+    mk = request.getfixturevalue(name)
+    g = np.load(os.path.join(HERE, "golden", "cv_ref.npz"))
+    T, flag = props_oracle.temperature_from_ea(mk["tables"], g[f"{name}_tea_ea"],
+                                               g[f"{name}_tea_rho"], g[f"{name}_tea_Y"],
+                                               g[f"{name}_tea_T0"])
+    assert np.array_equal(flag, g[f"{name}_tea_flag"])
+    assert np.abs(T - g[f"{name}_tea_T"]).max() < 1e-9

@@ -453,3 +453,19 @@ def test_temperature_from_enthalpy_vs_reference_golden(name, small, large):
     T, flag = m.temperature_from_enthalpy(d(g0["tha_ha"]), d(g0["prop_Y"]), d(g0["tha_T0"]))
     assert np.array_equal(flag.cpu().numpy(), g0["tha_flag"])
     assert np.abs(T.cpu().numpy() - g0["tha_T"]).max() < 1e-8
+
+
+@pytest.mark.parametrize("name", ["small", "ext"])
+def test_temperature_from_energy_vs_reference_golden(name, request):
+    """hc_temperature_from_energy against thermoList::TEa_rho's own outputs."""
+    import os
+    mk = request.getfixturevalue(name)
+    here = os.path.dirname(os.path.abspath(__file__))
+    g0 = np.load(os.path.join(here, "golden", "cv_ref.npz"))
+    dev = _cuda()
+    m = _mech(mk["tables"])
+    d = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+    T, flag = m.temperature_from_energy(d(g0[name + "_tea_ea"]), d(g0[name + "_tea_Y"]),
+                                        d(g0[name + "_tea_rho"]), d(g0[name + "_tea_T0"]))
+    assert np.array_equal(flag.cpu().numpy(), g0[name + "_tea_flag"])
+    assert np.abs(T.cpu().numpy() - g0[name + "_tea_T"]).max() < 1e-6
