@@ -398,6 +398,22 @@ int hc_source_terms_aos_async(hc_mech_t mech, int64_t n, const double *YiRhoT, c
                               double *RRi, void *stream);
 
 /*
+ * Mixture properties from records [Y_0..Y_{nsp-1}, T, p] (nsp + 2 doubles per
+ * cell), the input of CUDAThermo::calchaicp (thermo/include/thermoListCUDA.hpp:40-58,
+ * thermo/src/thermoListCUDA.cu:84-123) and CUDATransport::calcTransportProperties
+ * (transport/src/transportListCUDA.cu:236-276), into their outputs:
+ * haicp[cell * (nsp + 1) + i] = h_i [J/kg] and, at i = nsp, the mixture cp
+ * [J/kg/K]; DMuKappa[cell * (nsp + 2) + i] = D_i [m^2/s], then mu [Pa s] and
+ * kappa [W/m/K]. Either output may be NULL. hc_properties_aos takes device
+ * pointers (stream-ordered); hc_properties_aos_host host pointers
+ * (synchronous, as the reference's non-Async calls).
+ */
+int hc_properties_aos(hc_mech_t mech, int64_t n, const double *YiTP, double *haicp,
+                      double *DMuKappa, void *stream);
+int hc_properties_aos_host(hc_mech_t mech, int64_t n, const double *YiTP, double *haicp,
+                           double *DMuKappa, void *stream);
+
+/*
  * Measurement utility, no reference counterpart: runs an FP64 FMA-throughput
  * probe on the current device (independent FMA chains on every SM) and
  * returns the achieved TFLOP/s, the denominator of the integrator's roofline.

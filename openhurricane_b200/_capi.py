@@ -132,6 +132,8 @@ SIGNATURES = {
                               [C.c_int, _VP, _VP]),
     "hc_source_terms_aos": (C.c_int, [_VP, C.c_int64] + [_VP] * 3 + [_VP]),
     "hc_source_terms_aos_async": (C.c_int, [_VP, C.c_int64] + [_VP] * 3 + [_VP]),
+    "hc_properties_aos": (C.c_int, [_VP, C.c_int64] + [_VP] * 3 + [_VP]),
+    "hc_properties_aos_host": (C.c_int, [_VP, C.c_int64] + [_VP] * 3 + [_VP]),
     "hc_probe_fp64_peak": (C.c_int, [C.c_int, _VP, _VP]),
     "hc_mlp_create": (C.c_int, [C.c_int] * 5 + [C.c_uint64, C.POINTER(_VP)]),
     "hc_mlp_destroy": (C.c_int, [_VP]),

@@ -1156,6 +1156,84 @@ int hc_source_terms_aos_async(hc_mech_t m, int64_t n, const double *YiRhoT, cons
 
 }  // extern "C"
 
+// properties from records [Y..., T, p] (device pointers); rows is the
+// workspace: [nsp+2][n] input rows, [nsp+1][n] ha / cp rows, [nsp+2][n]
+// D / mu / kappa rows
+static int properties_records(hc_mech_t m, int64_t n, const double *recs, double *haicp,
+                              double *DMuKappa, double *rows, cudaStream_t st) {
+    const int nsp = m->dm.nsp;
+    const size_t nn = (size_t)n;
+    double *in = rows, *hc = in + nn * (nsp + 2), *dmk = hc + nn * (nsp + 1);
+    int rc = launch_records_to_rows(n, nsp + 2, recs, in, st, g_err);
+    if (rc != HC_OK) return rc;
+    const double *Y = in, *T = in + nn * nsp, *p = in + nn * (nsp + 1);
+    rc = launch_properties(m->dm, n, T, p, Y, haicp ? hc : nullptr, haicp ? hc + nn * nsp : nullptr,
+                           DMuKappa ? dmk + nn * nsp : nullptr,
+                           DMuKappa ? dmk + nn * (nsp + 1) : nullptr, DMuKappa ? dmk : nullptr, st,
+                           g_err);
+    if (rc != HC_OK) return rc;
+    if (haicp) {
+        rc = launch_rows_to_records(n, nsp + 1, nsp + 1, hc, haicp, nullptr, nsp, st, g_err);
+        if (rc != HC_OK) return rc;
+    }
+    if (DMuKappa)
+        rc = launch_rows_to_records(n, nsp + 2, nsp + 2, dmk, DMuKappa, nullptr, nsp, st, g_err);
+    return rc;
+}
+
+static int properties_records_check(hc_mech_t m, int64_t n, const void *recs, const void *a,
+                                    const void *b) {
+    if (!m) return fail(HC_E_INVALID, "null mechanism");
+    if (n < 0) return fail(HC_E_INVALID, "negative cell count");
+    if (n > 0 && (!recs || (!a && !b))) return fail(HC_E_INVALID, "null field");
+    if (m->dm.nsp + 2 > kAosMaxRec) return fail(HC_E_UNSUPPORTED, "too many species for records");
+    // the property kernel reads the transport tables (as hc_properties does)
+    if (!m->dm.geom || !m->dm.eps_k || !m->dm.sigma)
+        return fail(HC_E_INVALID, "mechanism has no transport data");
+    return HC_OK;
+}
+
+extern "C" {
+
+int hc_properties_aos(hc_mech_t m, int64_t n, const double *YiTP, double *haicp,
+                      double *DMuKappa, void *stream) {
+    int rc = properties_records_check(m, n, YiTP, haicp, DMuKappa);
+    if (rc != HC_OK || n == 0) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    std::lock_guard<std::mutex> lk(m->mu);
+    const size_t nn = (size_t)n, nsp = (size_t)m->dm.nsp;
+    rc = ensure_ws(m, sizeof(double) * nn * (3 * nsp + 5), st);
+    if (rc != HC_OK) return rc;
+    return properties_records(m, n, YiTP, haicp, DMuKappa, static_cast<double *>(m->ws), st);
+}
+
+int hc_properties_aos_host(hc_mech_t m, int64_t n, const double *YiTP, double *haicp,
+                           double *DMuKappa, void *stream) {
+    int rc = properties_records_check(m, n, YiTP, haicp, DMuKappa);
+    if (rc != HC_OK || n == 0) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    std::lock_guard<std::mutex> lk(m->mu);
+    const size_t nn = (size_t)n, nsp = (size_t)m->dm.nsp;
+    // rows (3 nsp + 5) n, then the records in (nsp + 2) n, ha / cp out (nsp + 1) n,
+    // D / mu / kappa out (nsp + 2) n
+    rc = ensure_ws(m, sizeof(double) * nn * (6 * nsp + 10), st);
+    if (rc != HC_OK) return rc;
+    double *rows = static_cast<double *>(m->ws);
+    double *rin = rows + nn * (3 * nsp + 5), *hout = rin + nn * (nsp + 2), *dout = hout + nn * (nsp + 1);
+    HC_CUDA(cudaMemcpyAsync(rin, YiTP, sizeof(double) * nn * (nsp + 2), cudaMemcpyHostToDevice, st));
+    rc = properties_records(m, n, rin, haicp ? hout : nullptr, DMuKappa ? dout : nullptr, rows, st);
+    if (rc != HC_OK) return rc;
+    if (haicp)
+        HC_CUDA(cudaMemcpyAsync(haicp, hout, sizeof(double) * nn * (nsp + 1), cudaMemcpyDeviceToHost, st));
+    if (DMuKappa)
+        HC_CUDA(cudaMemcpyAsync(DMuKappa, dout, sizeof(double) * nn * (nsp + 2), cudaMemcpyDeviceToHost,
+                                st));
+    HC_CUDA(cudaStreamSynchronize(st));
+    return HC_OK;
+}
+
+}  // extern "C"
+
 // ---------------------------------------------------------------------------
 // Allocation-free integration (hc_integrate_noalloc).
 //
