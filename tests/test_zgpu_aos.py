@@ -203,7 +203,8 @@ def test_property_records_match_species_major_fields(large):
     dmk = torch.empty((n, t.nsp + 2), dtype=torch.float64, device=dev)
     vp = lambda x: C.c_void_p(x.data_ptr())
     lib = _capi.load()
-    assert lib.hc_properties_aos(m.handle, n, vp(d(rec)), vp(hc), vp(dmk),
+    rec_d = d(rec)
+    assert lib.hc_properties_aos(m.handle, n, vp(rec_d), vp(hc), vp(dmk),
                                  C.c_void_p(torch.cuda.current_stream().cuda_stream)) == 0
     torch.cuda.synchronize()
     hc, dmk = hc.cpu().numpy(), dmk.cpu().numpy()
