@@ -408,6 +408,52 @@ int hc_source_terms_aos_async(hc_mech_t mech, int64_t n, const double *YiRhoT, c
  * pointers (stream-ordered); hc_properties_aos_host host pointers
  * (synchronous, as the reference's non-Async calls).
  */
+/* ------------------------------------------------------------------------
+ * Device state: a flow's cells resident on the device between calls, for
+ * callers that keep the fields there (hc_upload once, then integrate /
+ * source terms / properties every step, hc_download when the host needs
+ * them). The state owns device fields T[n], p[n], rho[n], Y[nsp*n]
+ * (species-major), the warm-start sub-steps subdt[n], Ri[nsp*n] and the
+ * per-cell statuses; hc_state_fields returns their device addresses. Calls
+ * are stream-ordered; downloads synchronise the stream. A state belongs to
+ * the mechanism it was made with, which must outlive it; record layouts go
+ * through the mechanism's workspace, so calls on one mechanism are issued
+ * on one stream.
+ */
+typedef struct hc_state_s *hc_state_t;
+
+/* record layouts (nsp + 2 doubles per cell) of the reference's CUDA path */
+#define HC_RECORDS_T_Y_RHO 0   /* [T, Y..., rho]: calcChemODEsArray */
+#define HC_RECORDS_Y_RHO_T 1   /* [Y..., rho, T]: calculateSourceTermsAsync (getYiRhoT) */
+#define HC_RECORDS_Y_T_P 2     /* [Y..., T, p]: calchaicp / calcTransportProperties */
+
+int hc_state_create(hc_mech_t mech, int64_t ncells, hc_state_t *out);
+int hc_state_destroy(hc_state_t state);
+int hc_state_fields(hc_state_t state, double **T, double **p, double **rho, double **Y,
+                    double **subdt, double **Ri, int32_t **status);
+/* host species-major fields in; any may be NULL (kept). Passing subdt sets the
+   warm-start sub-steps; otherwise the first integration starts from dt dtFactor. */
+int hc_upload(hc_state_t state, const double *T, const double *p, const double *rho,
+              const double *Y, const double *subdt, void *stream);
+/* host records in (HC_RECORDS_*); for layouts 0 and 1, p[n] (host) or NULL for
+   the ideal-gas pressure of the record's rho, T and Y */
+int hc_upload_records(hc_state_t state, int layout, const double *recs, const double *p,
+                      void *stream);
+/* host species-major fields out (any may be NULL); synchronises */
+int hc_download(hc_state_t state, double *T, double *rho, double *Y, double *Ri, double *subdt,
+                int32_t *status, void *stream);
+/* host records out, layout HC_RECORDS_T_Y_RHO or HC_RECORDS_Y_RHO_T; synchronises */
+int hc_download_records(hc_state_t state, int layout, double *recs, void *stream);
+/* one flow step of every cell over dt[n] (device) * dt_factor, as hc_integrate:
+   T, Y (and rho at constant pressure) updated, Ri, subdt and statuses written */
+int hc_state_integrate(hc_state_t state, const hc_opts *opts, const double *dt, double dt_factor,
+                       void *stream);
+/* Ri = omega_i W_i at the state's fields */
+int hc_state_source_terms(hc_state_t state, void *stream);
+/* mixture properties at the state's fields into device outputs (any may be NULL) */
+int hc_state_properties(hc_state_t state, double *ha, double *cp, double *mu, double *kappa,
+                        double *D, void *stream);
+
 int hc_properties_aos(hc_mech_t mech, int64_t n, const double *YiTP, double *haicp,
                       double *DMuKappa, void *stream);
 int hc_properties_aos_host(hc_mech_t mech, int64_t n, const double *YiTP, double *haicp,

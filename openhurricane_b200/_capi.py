@@ -133,6 +133,16 @@ SIGNATURES = {
     "hc_source_terms_aos": (C.c_int, [_VP, C.c_int64] + [_VP] * 3 + [_VP]),
     "hc_source_terms_aos_async": (C.c_int, [_VP, C.c_int64] + [_VP] * 3 + [_VP]),
     "hc_properties_aos": (C.c_int, [_VP, C.c_int64] + [_VP] * 3 + [_VP]),
+    "hc_state_create": (C.c_int, [_VP, C.c_int64, C.POINTER(_VP)]),
+    "hc_state_destroy": (C.c_int, [_VP]),
+    "hc_state_fields": (C.c_int, [_VP] + [_VP] * 7),
+    "hc_upload": (C.c_int, [_VP] + [_VP] * 5 + [_VP]),
+    "hc_upload_records": (C.c_int, [_VP, C.c_int, _VP, _VP, _VP]),
+    "hc_download": (C.c_int, [_VP] + [_VP] * 6 + [_VP]),
+    "hc_download_records": (C.c_int, [_VP, C.c_int, _VP, _VP]),
+    "hc_state_integrate": (C.c_int, [_VP, C.POINTER(HcOpts), _VP, C.c_double, _VP]),
+    "hc_state_source_terms": (C.c_int, [_VP, _VP]),
+    "hc_state_properties": (C.c_int, [_VP] + [_VP] * 5 + [_VP]),
     "hc_properties_aos_host": (C.c_int, [_VP, C.c_int64] + [_VP] * 3 + [_VP]),
     "hc_probe_fp64_peak": (C.c_int, [C.c_int, _VP, _VP]),
     "hc_mlp_create": (C.c_int, [C.c_int] * 5 + [C.c_uint64, C.POINTER(_VP)]),

@@ -94,6 +94,13 @@ __global__ void ideal_gas_p_kernel(int64_t n, int nsp, const double *__restrict_
     }
 }
 
+__global__ void scaled_copy_kernel(int64_t n, const double *__restrict__ src, double factor,
+                                   double *__restrict__ dst) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = src[i] * factor;
+}
+
 unsigned tiles_grid(int64_t n) {
     const int64_t tiles = (n + kAosTile - 1) / kAosTile;
     const int64_t cap = 148 * 16;
@@ -134,6 +141,16 @@ int launch_rows_to_records(int64_t n, int rec, int ncols, const double *rows, do
     rows_to_records_kernel<<<tiles_grid(n), kAosThreads, smem, st>>>(n, rec, ncols, rows, recs,
                                                                      W, nsp);
     return launched("rows_to_records_kernel", err);
+}
+
+// dst = src * factor (the first warm-start sub-steps, dtInit = dt dtFactor)
+int launch_scaled_copy(int64_t n, const double *src, double factor, double *dst, cudaStream_t st,
+                       std::string &err) {
+    if (n <= 0) return HC_OK;
+    const int64_t blocks = (n + 255) / 256;
+    scaled_copy_kernel<<<(unsigned)(blocks < 148 * 16 ? blocks : 148 * 16), 256, 0, st>>>(
+        n, src, factor, dst);
+    return launched("scaled_copy_kernel", err);
 }
 
 int launch_ideal_gas_p(int64_t n, int nsp, const double *W, const double *T, const double *rho,

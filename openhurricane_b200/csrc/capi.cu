@@ -1235,6 +1235,228 @@ int hc_properties_aos_host(hc_mech_t m, int64_t n, const double *YiTP, double *h
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
+// Device state: the fields of a flow's cells resident on the device between
+// calls (T, p, rho, Y, the warm-start sub-steps, Ri, per-cell statuses), with
+// uploads and downloads in species-major or record-per-cell layouts. One
+// allocation laid out [T][Y][rho][p][subdt][Ri][status], so that integration
+// records [T, Y..., rho] transpose straight into the first nsp + 2 rows.
+// ---------------------------------------------------------------------------
+struct hc_state_s {
+    hc_mech_t m = nullptr;
+    int64_t n = 0;
+    void *block = nullptr;
+    double *T = nullptr, *Y = nullptr, *rho = nullptr, *p = nullptr, *subdt = nullptr;
+    double *Ri = nullptr;
+    int32_t *status = nullptr;
+    bool warm = false;   // subdt holds warm-start sub-steps
+};
+
+namespace {
+
+int state_check(hc_state_t s) {
+    if (!s || !s->m) return fail(HC_E_INVALID, "null state");
+    return HC_OK;
+}
+
+// records (device) of one of the HC_RECORDS_* layouts -> the state's fields
+int state_from_records(hc_state_t s, int layout, const double *recs, cudaStream_t st) {
+    hc_mech_t m = s->m;
+    const int nsp = m->dm.nsp;
+    const size_t n = (size_t)s->n;
+    if (layout == HC_RECORDS_T_Y_RHO) return launch_records_to_rows(s->n, nsp + 2, recs, s->T, st, g_err);
+    int rc = ensure_ws(m, sizeof(double) * n * (nsp + 2), st);
+    if (rc != HC_OK) return rc;
+    double *rows = static_cast<double *>(m->ws);
+    rc = launch_records_to_rows(s->n, nsp + 2, recs, rows, st, g_err);
+    if (rc != HC_OK) return rc;
+    HC_CUDA(cudaMemcpyAsync(s->Y, rows, sizeof(double) * n * nsp, cudaMemcpyDeviceToDevice, st));
+    double *a = (layout == HC_RECORDS_Y_RHO_T) ? s->rho : s->T;
+    double *b = (layout == HC_RECORDS_Y_RHO_T) ? s->T : s->p;
+    HC_CUDA(cudaMemcpyAsync(a, rows + n * nsp, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    HC_CUDA(cudaMemcpyAsync(b, rows + n * (nsp + 1), sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    return HC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hc_state_create(hc_mech_t m, int64_t ncells, hc_state_t *out) {
+    if (!out) return fail(HC_E_INVALID, "null argument");
+    *out = nullptr;
+    if (!m) return fail(HC_E_INVALID, "null mechanism");
+    if (ncells < 1) return fail(HC_E_INVALID, "a state holds at least one cell");
+    const size_t n = (size_t)ncells, nsp = (size_t)m->dm.nsp;
+    const size_t doubles = n * (4 + 2 * nsp + 1);   // T, Y, rho, p, subdt, Ri
+    void *b = nullptr;
+    HC_CUDA(cudaMalloc(&b, sizeof(double) * doubles + sizeof(int32_t) * n));
+    hc_state_s *s = new hc_state_s();
+    s->m = m;
+    s->n = ncells;
+    s->block = b;
+    double *q = static_cast<double *>(b);
+    s->T = q;
+    s->Y = q + n;
+    s->rho = s->Y + n * nsp;
+    s->p = s->rho + n;
+    s->subdt = s->p + n;
+    s->Ri = s->subdt + n;
+    s->status = reinterpret_cast<int32_t *>(s->Ri + n * nsp);
+    cudaError_t e = cudaMemset(b, 0, sizeof(double) * doubles + sizeof(int32_t) * n);
+    if (e != cudaSuccess) {
+        cudaFree(b);
+        delete s;
+        return fail(HC_E_CUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
+    }
+    *out = s;
+    return HC_OK;
+}
+
+int hc_state_destroy(hc_state_t s) {
+    if (!s) return HC_OK;
+    if (s->block) cudaFree(s->block);
+    delete s;
+    return HC_OK;
+}
+
+int hc_state_fields(hc_state_t s, double **T, double **p, double **rho, double **Y,
+                    double **subdt, double **Ri, int32_t **status) {
+    int rc = state_check(s);
+    if (rc != HC_OK) return rc;
+    if (T) *T = s->T;
+    if (p) *p = s->p;
+    if (rho) *rho = s->rho;
+    if (Y) *Y = s->Y;
+    if (subdt) *subdt = s->subdt;
+    if (Ri) *Ri = s->Ri;
+    if (status) *status = s->status;
+    return HC_OK;
+}
+
+int hc_upload(hc_state_t s, const double *T, const double *p, const double *rho, const double *Y,
+              const double *subdt, void *stream) {
+    int rc = state_check(s);
+    if (rc != HC_OK) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t n = (size_t)s->n, nsp = (size_t)s->m->dm.nsp;
+    if (T) HC_CUDA(cudaMemcpyAsync(s->T, T, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    if (p) HC_CUDA(cudaMemcpyAsync(s->p, p, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    if (rho) HC_CUDA(cudaMemcpyAsync(s->rho, rho, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    if (Y) HC_CUDA(cudaMemcpyAsync(s->Y, Y, sizeof(double) * n * nsp, cudaMemcpyHostToDevice, st));
+    if (subdt) {
+        HC_CUDA(cudaMemcpyAsync(s->subdt, subdt, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+        s->warm = true;
+    }
+    return HC_OK;
+}
+
+int hc_upload_records(hc_state_t s, int layout, const double *recs, const double *p,
+                      void *stream) {
+    int rc = state_check(s);
+    if (rc != HC_OK) return rc;
+    if (layout < HC_RECORDS_T_Y_RHO || layout > HC_RECORDS_Y_T_P)
+        return fail(HC_E_INVALID, "unknown record layout");
+    if (!recs) return fail(HC_E_INVALID, "null records");
+    hc_mech_t m = s->m;
+    if (m->dm.nsp + 2 > kAosMaxRec) return fail(HC_E_UNSUPPORTED, "too many species for records");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t n = (size_t)s->n, rec = (size_t)m->dm.nsp + 2;
+    std::lock_guard<std::mutex> lk(m->mu);
+    // the host records are staged in the mechanism's workspace behind the rows
+    // the transpose of layouts 1 and 2 uses
+    rc = ensure_ws(m, sizeof(double) * n * 2 * rec, st);
+    if (rc != HC_OK) return rc;
+    double *stage = static_cast<double *>(m->ws) + n * rec;
+    HC_CUDA(cudaMemcpyAsync(stage, recs, sizeof(double) * n * rec, cudaMemcpyHostToDevice, st));
+    rc = state_from_records(s, layout, stage, st);
+    if (rc != HC_OK) return rc;
+    if (layout == HC_RECORDS_Y_T_P) return HC_OK;   // p came with the records
+    if (p) {
+        HC_CUDA(cudaMemcpyAsync(s->p, p, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+        return HC_OK;
+    }
+    return launch_ideal_gas_p(s->n, m->dm.nsp, m->dm.W, s->T, s->rho, s->Y, s->p, st, g_err);
+}
+
+int hc_download(hc_state_t s, double *T, double *rho, double *Y, double *Ri, double *subdt,
+                int32_t *status, void *stream) {
+    int rc = state_check(s);
+    if (rc != HC_OK) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t n = (size_t)s->n, nsp = (size_t)s->m->dm.nsp;
+    if (T) HC_CUDA(cudaMemcpyAsync(T, s->T, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    if (rho) HC_CUDA(cudaMemcpyAsync(rho, s->rho, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    if (Y) HC_CUDA(cudaMemcpyAsync(Y, s->Y, sizeof(double) * n * nsp, cudaMemcpyDeviceToHost, st));
+    if (Ri) HC_CUDA(cudaMemcpyAsync(Ri, s->Ri, sizeof(double) * n * nsp, cudaMemcpyDeviceToHost, st));
+    if (subdt) HC_CUDA(cudaMemcpyAsync(subdt, s->subdt, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    if (status)
+        HC_CUDA(cudaMemcpyAsync(status, s->status, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st));
+    HC_CUDA(cudaStreamSynchronize(st));
+    return HC_OK;
+}
+
+int hc_download_records(hc_state_t s, int layout, double *recs, void *stream) {
+    int rc = state_check(s);
+    if (rc != HC_OK) return rc;
+    if (layout != HC_RECORDS_T_Y_RHO && layout != HC_RECORDS_Y_RHO_T)
+        return fail(HC_E_INVALID, "records of T, Y and rho are layouts 0 and 1");
+    if (!recs) return fail(HC_E_INVALID, "null records");
+    hc_mech_t m = s->m;
+    if (m->dm.nsp + 2 > kAosMaxRec) return fail(HC_E_UNSUPPORTED, "too many species for records");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t n = (size_t)s->n, nsp = (size_t)m->dm.nsp, rec = nsp + 2;
+    std::lock_guard<std::mutex> lk(m->mu);
+    rc = ensure_ws(m, sizeof(double) * n * 2 * rec, st);
+    if (rc != HC_OK) return rc;
+    double *rows = static_cast<double *>(m->ws), *out = rows + n * rec;
+    const double *src = s->T;
+    if (layout == HC_RECORDS_Y_RHO_T) {
+        HC_CUDA(cudaMemcpyAsync(rows, s->Y, sizeof(double) * n * nsp, cudaMemcpyDeviceToDevice, st));
+        HC_CUDA(cudaMemcpyAsync(rows + n * nsp, s->rho, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        HC_CUDA(cudaMemcpyAsync(rows + n * (nsp + 1), s->T, sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                                st));
+        src = rows;
+    }
+    rc = launch_rows_to_records(s->n, (int)rec, (int)rec, src, out, nullptr, (int)nsp, st, g_err);
+    if (rc != HC_OK) return rc;
+    HC_CUDA(cudaMemcpyAsync(recs, out, sizeof(double) * n * rec, cudaMemcpyDeviceToHost, st));
+    HC_CUDA(cudaStreamSynchronize(st));
+    return HC_OK;
+}
+
+int hc_state_integrate(hc_state_t s, const hc_opts *opts, const double *dt, double dt_factor,
+                       void *stream) {
+    int rc = state_check(s);
+    if (rc != HC_OK) return rc;
+    if (!dt) return fail(HC_E_INVALID, "null dt");
+    if (!(dt_factor > 0)) return fail(HC_E_INVALID, "dt_factor must be positive");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (!s->warm) {
+        // the first flow step starts from dtInit = dt dtFactor (chemistrySource.inl:86-95)
+        rc = launch_scaled_copy(s->n, dt, dt_factor, s->subdt, st, g_err);
+        if (rc != HC_OK) return rc;
+        s->warm = true;
+    }
+    return integrate_impl(s->m, opts, s->n, s->T, s->p, s->rho, s->Y, dt, dt_factor, s->subdt,
+                          s->Ri, s->status, nullptr, nullptr, st);
+}
+
+int hc_state_source_terms(hc_state_t s, void *stream) {
+    int rc = state_check(s);
+    if (rc != HC_OK) return rc;
+    return hc_source_terms(s->m, s->n, s->T, s->p, s->rho, s->Y, s->Ri, stream);
+}
+
+int hc_state_properties(hc_state_t s, double *ha, double *cp, double *mu, double *kappa, double *D,
+                        void *stream) {
+    int rc = state_check(s);
+    if (rc != HC_OK) return rc;
+    return hc_properties(s->m, s->n, s->T, s->p, s->Y, ha, cp, mu, kappa, D, stream);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
 // Allocation-free integration (hc_integrate_noalloc).
 //
 // For callers that must not allocate device memory during the call: a flow

@@ -64,4 +64,6 @@ int launch_rows_to_records(int64_t n, int rec, int ncols, const double *rows, do
                            const double *W, int nsp, cudaStream_t st, std::string &err);
 int launch_ideal_gas_p(int64_t n, int nsp, const double *W, const double *T, const double *rho,
                        const double *Y, double *p, cudaStream_t st, std::string &err);
+int launch_scaled_copy(int64_t n, const double *src, double factor, double *dst, cudaStream_t st,
+                       std::string &err);
 }

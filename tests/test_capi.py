@@ -83,3 +83,15 @@ def test_mechanism_checks_of_the_extended_rate_forms_without_gpu(ext):
     def bad_code(b):
         b.arrays["reversible"][0] = 3
     bad(bad_code, b"reversibility")
+
+
+def test_state_api_rejects_null_handles_without_gpu():
+    from openhurricane_b200 import _capi
+    lib = _capi.load()
+    st = C.c_void_p()
+    assert lib.hc_state_create(None, 16, C.byref(st)) == -1
+    assert b"null mechanism" in lib.hc_last_error()
+    assert lib.hc_upload(None, None, None, None, None, None, None) == -1
+    assert lib.hc_download(None, None, None, None, None, None, None, None) == -1
+    assert lib.hc_state_integrate(None, C.byref(_capi.default_opts()), None, 1.0, None) == -1
+    assert lib.hc_state_destroy(None) == 0
