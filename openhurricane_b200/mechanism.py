@@ -31,8 +31,8 @@ order, as the reference so that the tables hold identical bits:
   order of a side taken from its reaction orders (after FORD / RORD).
 
 Supported rate forms: Arrhenius, Arrhenius third-body (+M), unimolecular
-fall-off (+M) with Lindemann, Troe (3 or 4 parameters) or SRI (3 or 5
-parameters); reversible (=, <=>) and irreversible (=>) reactions; explicit
+fall-off (+M, or a named third body +X) with Lindemann, Troe (3 or 4
+parameters) or SRI (3 or 5 parameters); reversible (=, <=>) and irreversible (=>) reactions; explicit
 reverse Arrhenius parameters (REV, reversibleReactionWithRevPars) on
 Arrhenius and third-body reactions; non-stoichiometric orders (FORD, RORD).
 pressure-dependent Arrhenius tables (PLOG, logInterpolationRR) on reactions
@@ -118,6 +118,7 @@ class ParsedReaction:
     plog: Optional[List[Tuple[float, float, float, float]]] = None   # (p atm, A, b, E) as read
     high: Optional[Tuple[float, float, float]] = None   # HIGH A, b, E (chemically activated)
     lt: Optional[Tuple[float, float]] = None             # Landau-Teller B, C
+    named_third: Optional[int] = None                    # species of a (+X) third body
 
 
 @dataclasses.dataclass
@@ -262,10 +263,15 @@ def parse_chemkin(che_text: str, species_names: Optional[List[str]] = None):
             A, b, E = _read_real(m.group(4)), _read_real(m.group(5)), _read_real(m.group(6))
             kind = "arrhenius"
             pd = re.compile(r"\(\s*\+\s*(\S+?)\s*\)")
+            third = None
             if pd.search(lhs) or pd.search(rhs):
-                third = pd.search(lhs).group(1)
-                if third.upper() != "M":
-                    raise NotImplementedError("species-specific (+X) fall-off")
+                tl, tr = pd.search(lhs), pd.search(rhs)
+                if not (tl and tr) or tl.group(1) != tr.group(1):
+                    raise ValueError(f"pressure-dependent reaction with unmatched third bodies: "
+                                     f"{line.strip()!r}")
+                third = tl.group(1)
+                if third.upper() != "M" and third not in index:
+                    raise ValueError(f"third body {third!r} is not a species")
                 lhs, rhs = pd.sub("", lhs), pd.sub("", rhs)
                 kind = "falloff"
             tb = re.compile(r"\+\s*M(?![-a-zA-Z0-9])", re.IGNORECASE)
@@ -277,6 +283,13 @@ def parse_chemkin(che_text: str, species_names: Optional[List[str]] = None):
                                  units_A=units["A"], units_E=units["E"])
             if kind in ("third_body", "falloff"):
                 cur.eff = np.ones(len(names))
+            if third is not None and third.upper() != "M":
+                # a named third body (+X): efficiency 1 for X, 0 for every other
+                # species (chemkinFileRead.cpp:1002-1061); an efficiency line may
+                # then name X only (chemkinFileRead.cpp:797-822)
+                cur.eff = np.zeros(len(names))
+                cur.eff[index[third]] = 1.0
+                cur.named_third = index[third]
             reactions.append(cur)
             continue
         # auxiliary line: KEY / values / groups, bare words, species efficiencies
@@ -356,6 +369,9 @@ def parse_chemkin(che_text: str, species_names: Optional[List[str]] = None):
             else:
                 if key not in index:
                     raise ValueError(f"unknown efficiency species {key!r}")
+                if cur.named_third is not None and index[key] != cur.named_third:
+                    raise ValueError(f"the third body of this reaction is "
+                                     f"{names[cur.named_third]}, but {key} has an efficiency")
                 if cur.eff is None:
                     raise ValueError(f"efficiencies on a reaction without a third body: {line!r}")
                 cur.eff[index[key]] = _read_real(val)

@@ -74,3 +74,46 @@ def test_example_mechanism_known_answers_match_the_reference():
     dydt, J = port.rhs_jac(port.MechDesc(t), c, T, p)
     assert np.array_equal(dydt, k["dydt"])
     assert np.array_equal(J, k["J"])
+
+
+def test_named_third_body_falloff_matches_the_reference(small, tmp_path):
+    """A fall-off reaction with a named third body, (+N2): efficiency 1 for N2
+    and 0 for the others (chemkinFileRead.cpp:1002-1061), through the reader
+    and the oracle against the reference build."""
+    from openhurricane_b200 import mechanism, synth
+    from oracle import port, refrun
+    if not refrun.available():
+        pytest.skip("reference binary not built (make -f oracle/Makefile.ref)")
+    che, th, tr = small["files"]
+    txt = open(che).read()
+    assert "(+M)" in txt
+    # the reaction's efficiency line is dropped: with a named third body the
+    # reference takes an efficiency for that species only
+    lines, out, skip = txt.replace("(+M)", "(+N2)").splitlines(), [], False
+    for line in lines:
+        if "(+N2)" in line:
+            skip = True
+        elif skip and "/" in line and not line.strip().upper().startswith(("LOW", "TROE")):
+            continue
+        elif "=" in line:
+            skip = False
+        out.append(line)
+    che2 = str(tmp_path / "named.che")
+    with open(che2, "w") as f:
+        f.write("\n".join(out) + "\n")
+    t = mechanism.compile_mechanism(che2, th, tr)
+    r = int(np.flatnonzero(t.rate_type >= mechanism.RATE_LINDEMANN)[0])
+    assert t.eff[r, t.names.index("N2")] == 1.0 and t.eff[r].sum() == 1.0
+    with pytest.raises(ValueError, match="third body"):
+        with open(str(tmp_path / "bad.che"), "w") as f:
+            f.write(txt.replace("(+M)", "(+N2)"))
+        mechanism.compile_mechanism(str(tmp_path / "bad.che"), th, tr)
+    case = str(tmp_path / "case.cont")
+    refrun.write_case(case, che2, th, tr, {"atol": 1e-15})
+    c = synth.dirichlet_cells(t.nsp, 8, seed=303)
+    rho = synth.mixture_density(t.W, c)
+    ref = refrun.integrate(case, c.T, c.p, rho, 1e-6, 1e-6, c.Y, procs=4, workdir=str(tmp_path))
+    o = port.integrate(port.MechDesc(t), c.T, c.p, rho, c.Y, 1e-6,
+                       opts=port.default_opts(atol=1e-15))
+    for k in ("T", "Y", "rho", "c", "subdt"):
+        assert np.array_equal(o[k], ref[k]), k
