@@ -434,14 +434,33 @@ def parse_transport(text: str, names: List[str]):
     return out
 
 
-def compile_mechanism(che_path: str, thermo_path: str, transport_path: str) -> MechTables:
+def _embedded(che: str, start_re: str) -> str:
+    """A THERMO or TRANSPORT section carried in the mechanism file itself, used
+    when no separate file is given (chemkinFileRead.cpp:1700-1718, 1730-1739)."""
+    m = re.search(start_re + r"\s+[\s\S]*?\s+END", _strip_comments(che), re.IGNORECASE)
+    return m.group(0) if m else ""
+
+
+def compile_mechanism(che_path: str, thermo_path: Optional[str] = None,
+                      transport_path: Optional[str] = None) -> MechTables:
+    """Tables from a Chemkin mechanism file and its NASA-7 thermo and transport
+    files; without a thermo or transport file, the mechanism file's own
+    THERMO / TRANSPORT section is read, as the reference does."""
     with open(che_path) as f:
         che = f.read()
     names, elements, reactions = parse_chemkin(che)
-    with open(thermo_path) as f:
-        thermo = parse_thermo(f.read(), names)
-    with open(transport_path) as f:
-        tran = parse_transport(f.read(), names)
+    if thermo_path:
+        with open(thermo_path) as f:
+            thermo_txt = f.read()
+    else:
+        thermo_txt = _embedded(che, r"THER(?:MO|)")
+    thermo = parse_thermo(thermo_txt, names)
+    if transport_path:
+        with open(transport_path) as f:
+            tran_txt = f.read()
+    else:
+        tran_txt = _embedded(che, r"TRAN(?:SPORT|)")
+    tran = parse_transport(tran_txt, names)
     nsp, nrc = len(names), len(reactions)
 
     W = np.zeros(nsp)

@@ -178,3 +178,18 @@ def test_plog_tables_are_sorted_and_converted(ext, tmp_path):
     f.write_text(che)
     with pytest.raises(ValueError, match="highest pressure"):
         M.compile_mechanism(str(f), *ext["files"][1:])
+
+
+def test_thermo_and_transport_sections_in_the_mechanism_file(small, tmp_path):
+    """Without separate files, the THERMO and TRANSPORT sections of the
+    mechanism file are read (as the reference's reader does) and give the same
+    tables."""
+    che, th, tr = small["files"]
+    txt = open(che).read() + "\nTHERMO\n" + open(th).read().split("THERMO", 1)[1] + \
+        "\nTRANSPORT\n" + open(tr).read() + "END\n"
+    one = tmp_path / "all_in_one.che"
+    one.write_text(txt)
+    a = small["tables"]
+    b = M.compile_mechanism(str(one))
+    for k in ("W", "nasa", "Trange", "arr", "arr0", "troe", "eff", "geom", "eps_k", "sigma"):
+        assert np.array_equal(getattr(a, k), getattr(b, k)), k
