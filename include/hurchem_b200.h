@@ -176,6 +176,10 @@ void hc_default_opts(hc_opts *opts);
  * must precede any stream capture), 4 = compact thread per cell (mechanism
  * in the kernel's constant parameter bank: nsp <= 15, <= 64 reactions);
  * block = threads per block of the thread-per-cell kernels (32, 64 or 128). Set by the autotuner (openhurricane_b200/autotune.py).
+ * The thread-per-cell kernels (1, 3, 4) take nsp <= 15, the constant-pressure
+ * reactor and the common rate forms (Arrhenius, third body, Lindemann / Troe
+ * fall-off); a call that asks for one of them outside that range fails with
+ * HC_E_UNSUPPORTED. The cell group takes everything hc_mech_create accepts.
  * No reference counterpart.
  */
 int hc_set_tuning(hc_mech_t mech, int kernel, int block);
