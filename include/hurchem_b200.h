@@ -59,6 +59,8 @@ extern "C" {
                                interpolation, Chemkin PLOG (logInterpolationRR) */
 #define HC_RATE_LANDAU_TELLER 7   /* A T^b exp(-Ta/T + B/T^(1/3) + C/T^(2/3)), Chemkin LT
                                      (LandauTellerRR) */
+#define HC_RATE_JANEV 8     /* A T^b exp(-Ta/T + sum_{n<9} b_n (ln T)^n), Chemkin JAN (JanevRR) */
+#define HC_RATE_POWER_SERIES 9  /* A T^b exp(sum_{n<4} b_n / T^(n+1)), Chemkin FIT1 (powerSeriesRR) */
 
 /* hc_mech_desc.reversible */
 #define HC_IRREVERSIBLE 0
@@ -116,6 +118,8 @@ typedef struct hc_mech_desc {
        line) and arr = kinf (HIGH); k = k0 F / (1 + Pr). NULL: none */
     const int32_t *activated; /* [nrc] */
     const double *lt;        /* [nrc*2] Landau-Teller B, C (HC_RATE_LANDAU_TELLER); NULL: none */
+    const double *xcoef;     /* [nrc*9] Janev b_0..b_8 or power-series b_0..b_3 (then zeros);
+                                NULL: none */
 } hc_mech_desc;
 
 /*

@@ -199,10 +199,11 @@ static void make_host(const hc_mech_desc *d, HostMech &h) {
     const std::vector<double> zeros2((size_t)nrc * 2, 0.0);
     h.activated = permute(d->activated ? d->activated : zeros1i.data(), 1);
     h.lt = permute(d->lt ? d->lt : zeros2.data(), 2);
+    const std::vector<double> zeros9((size_t)nrc * 9, 0.0);
+    h.xcoef = permute(d->xcoef ? d->xcoef : zeros9.data(), 9);
     h.ext = false;
     for (int r = 0; r < nrc; ++r)
-        if (d->rate_type[r] == HC_RATE_SRI || d->rate_type[r] == HC_RATE_PLOG ||
-            d->rate_type[r] == HC_RATE_LANDAU_TELLER || d->reversible[r] == HC_REVERSIBLE_REV ||
+        if (d->rate_type[r] >= HC_RATE_SRI || d->reversible[r] == HC_REVERSIBLE_REV ||
             (d->activated && d->activated[r]))
             h.ext = true;
     // PLOG tables follow their reactions into device order
@@ -289,8 +290,13 @@ static int check_desc(const hc_mech_desc *d) {
     for (int r = 0; r < nrc; ++r) {
         if (d->nf[r] < 0 || d->nf[r] > HC_MAX_SIDE || d->nb[r] < 0 || d->nb[r] > HC_MAX_SIDE)
             return fail(HC_E_INVALID, "reaction side larger than HC_MAX_SIDE");
-        if (d->rate_type[r] < 0 || d->rate_type[r] > HC_RATE_LANDAU_TELLER)
+        if (d->rate_type[r] < 0 || d->rate_type[r] > HC_RATE_POWER_SERIES)
             return fail(HC_E_INVALID, "unknown rate type");
+        if (d->rate_type[r] >= HC_RATE_JANEV) {
+            if (!d->xcoef) return fail(HC_E_INVALID, "Janev / power-series reaction without coefficients");
+            if (d->reversible[r] == HC_REVERSIBLE_REV)
+                return fail(HC_E_INVALID, "explicit reverse parameters on a Janev / power-series reaction");
+        }
         if (d->activated && d->activated[r] &&
             (d->rate_type[r] < HC_RATE_LINDEMANN || d->rate_type[r] > HC_RATE_SRI))
             return fail(HC_E_INVALID, "chemically activated reaction without a fall-off form");
@@ -427,6 +433,7 @@ int hc_mech_create(const hc_mech_desc *d, hc_mech_t *out) {
     up(hm.arr_rev.data(), 3 * (size_t)nrc, &dm.arr_rev);
     up(hm.activated.data(), (size_t)nrc, &dm.activated);
     up(hm.lt.data(), 2 * (size_t)nrc, &dm.lt);
+    up(hm.xcoef.data(), 9 * (size_t)nrc, &dm.xcoef);
     up(hm.plog_ptr.data(), (size_t)nrc + 1, &dm.plog_ptr);
     up(hm.plog_p.data(), hm.plog_p.size(), &dm.plog_p);
     up(hm.plog_arr.data(), hm.plog_arr.size(), &dm.plog_arr);
@@ -534,7 +541,7 @@ int hc_jit_source(const hc_mech_desc *d, int block, char *buf, int64_t cap, int6
     make_host(d, h);
     if (h.ext)
         return fail(HC_E_UNSUPPORTED,
-                    "no generated kernel for SRI, explicit reverse (REV), PLOG, HIGH or LT rate laws");
+                    "no generated kernel for SRI, explicit reverse (REV), PLOG, HIGH, LT, JAN or FIT1 rate laws");
     const std::string src = jit_t1_source(h, block);
     *len = (int64_t)src.size();
     if (buf && cap > 0) {
@@ -597,13 +604,13 @@ static int integrate_impl(hc_mech_t m, const hc_opts *opts, int64_t ncells, doub
     if (m->kernel == 1 && !t1_ok)
         return fail(HC_E_UNSUPPORTED,
                     "thread-per-cell kernel needs nsp <= 15, autoUpdateJacobian off, the "
-                    "constant-pressure reactor and no SRI or explicit reverse (REV), PLOG, HIGH or "
-                    "LT rate laws");
+                    "constant-pressure reactor and no SRI or explicit reverse (REV), PLOG, HIGH, "
+                    "LT, JAN or FIT1 rate laws");
     if (m->kernel == 4 && !(t1_ok && m->t2_ok))
         return fail(HC_E_UNSUPPORTED,
                     "compact thread-per-cell kernel needs nsp <= 15, <= 64 reactions, "
                     "autoUpdateJacobian off, the constant-pressure reactor and no SRI, explicit "
-                    "reverse (REV), PLOG, HIGH or LT rate laws");
+                    "reverse (REV), PLOG, HIGH, LT, JAN or FIT1 rate laws");
     // automatic choice: the cell group. Per-cell costs in a flow step differ
     // by orders of magnitude, and the step lasts as long as its stiffest
     // cell; the cell group's lanes share each Newton iteration's work and
@@ -627,8 +634,8 @@ static int integrate_impl(hc_mech_t m, const hc_opts *opts, int64_t ncells, doub
     if (m->kernel == 3 && !t1_ok)
         return fail(HC_E_UNSUPPORTED,
                     "generated thread-per-cell kernel needs nsp <= 15, autoUpdateJacobian off, the "
-                    "constant-pressure reactor and no SRI, explicit reverse (REV), PLOG, HIGH or LT "
-                    "rate laws");
+                    "constant-pressure reactor and no SRI, explicit reverse (REV), PLOG, HIGH, LT, "
+                    "JAN or FIT1 rate laws");
     bool use_jit = t1_ok && m->kernel == 3;
     if (use_jit && !m->jit_tried) {
         // first use: generate, compile and load (host work, no stream operation)
@@ -1507,8 +1514,8 @@ extern "C" int hc_integrate_noalloc(hc_mech_t m, const hc_opts *opts, int64_t nc
     if (N > 16 || opts->auto_update_jacobian || !m->t2_ok || opts->reactor != 0)
         return fail(HC_E_UNSUPPORTED,
                     "hc_integrate_noalloc needs nsp <= 15, <= 64 reactions, autoUpdateJacobian off, "
-                    "the constant-pressure reactor and no SRI, explicit reverse (REV), PLOG, HIGH or "
-                    "LT rate laws");
+                    "the constant-pressure reactor and no SRI, explicit reverse (REV), PLOG, HIGH, "
+                    "LT, JAN or FIT1 rate laws");
     int dev = -1;
     HC_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 256) return fail(HC_E_CUDA, "device ordinal out of range");

@@ -194,7 +194,8 @@ struct CellCtx {
             bo[k] = (k < nb) ? ldg(&m.bord[kMaxSide * r + k]) : 0.0;
         }
         double M = 0.0;
-        if (type != kArrhenius && !(X && (type == kPLOG || type == kLandauTeller))) {
+        // PLOG, Landau-Teller, Janev and power series (codes 6 and up) carry no third body
+        if (type != kArrhenius && !(X && type >= kPLOG)) {
             const double *e = &m.eff[(int64_t)r * nsp];
             for (int i = 0; i < nsp; ++i) M += ldg(&e[i]) * c[i];
         }
@@ -208,6 +209,8 @@ struct CellCtx {
             kf = plog_k_global(m.plog_ptr, m.plog_p, m.plog_arr, r, p, T, logT);
         } else if (X && type == kLandauTeller) {
             kf = lt_k_global(&m.arr[3 * r], &m.lt[2 * r], T, logT);
+        } else if (X && type >= kJanev) {
+            kf = xrate_k_global(type, &m.arr[3 * r], &m.xcoef[9 * r], T, logT);
         } else {
             const double A0 = ldg(&m.arr0[3 * r]);
             b0 = ldg(&m.arr0[3 * r + 1]);
@@ -309,6 +312,8 @@ struct CellCtx {
             dkfdT = plog_dkdt_global(m.plog_ptr, m.plog_p, m.plog_arr, r, kf, p, T, logT);
         } else if (X && type == kLandauTeller) {
             dkfdT = lt_dkdt_global(&m.arr[3 * r], &m.lt[2 * r], kf, T);
+        } else if (X && type >= kJanev) {
+            dkfdT = xrate_dkdt_global(type, &m.arr[3 * r], &m.xcoef[9 * r], kf, T, logT);
         } else if (X && ldg(&m.activated[r])) {
             dkfdT = (1.0 / (1.0 + Pr)) * F * (k0 * invT * (b0 + Ta0 * invT));
         } else {
@@ -334,7 +339,7 @@ struct CellCtx {
         if (type == kThirdBody) {
             kind = 1.0;
             rec[11] = q / hmax(M, kTiny);
-        } else if (type != kArrhenius && !(X && (type == kPLOG || type == kLandauTeller))) {
+        } else if (type != kArrhenius && !(X && type >= kPLOG)) {
             if (M > kTiny) {
                 // unimolecularFallOffRR::gamDGamDT (unimolecularFallOffRR.cpp:55-91)
                 const double Pr2 = k0 * M / notZeroD(kinf);

@@ -21,6 +21,7 @@ struct HostMech {
     std::vector<double> sri, arr_rev;
     std::vector<int32_t> activated;        // [nrc] chemically activated bimolecular
     std::vector<double> lt;                // [nrc*2] Landau-Teller B, C
+    std::vector<double> xcoef;             // [nrc*9] Janev / power-series coefficients
     std::vector<int32_t> plog_ptr;         // [nrc+1], in device reaction order
     std::vector<double> plog_p, plog_arr;
     // the mechanism uses rate forms only the cell-group kernels evaluate

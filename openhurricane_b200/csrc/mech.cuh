@@ -23,6 +23,7 @@ struct DevMech {
     int32_t ext;                      // any SRI, REV, PLOG, HIGH or LT reaction
     const int32_t *activated;         // [nrc] chemically activated bimolecular (HIGH)
     const double *lt;                 // [nrc*2] Landau-Teller B, C
+    const double *xcoef;              // [nrc*9] Janev / power-series coefficients
     const int32_t *plog_ptr;          // [nrc+1] PLOG entries of each reaction
     const double *plog_p, *plog_arr;  // [n] Pa, [n*3] A, beta, Ta
     const double *eff;      // [nrc*nsp]
@@ -148,6 +149,23 @@ static __device__ __noinline__ double lt_k_global(const double *a, const double 
 static __device__ __noinline__ double lt_dkdt_global(const double *a, const double *bc, double k,
                                                     double T) {
     return lt_dkdt(k, ldg(&a[1]), ldg(&a[2]), ldg(&bc[0]), ldg(&bc[1]), T);
+}
+
+// Janev and power-series rates: a = A, beta, Ta; x = the reaction's 9 coefficients
+static __device__ __noinline__ double xrate_k_global(int type, const double *a, const double *x,
+                                                    double T, double logT) {
+    double bn[9];
+    for (int n = 0; n < 9; ++n) bn[n] = ldg(&x[n]);
+    if (type == kJanev) return janev_k(ldg(&a[0]), ldg(&a[1]), ldg(&a[2]), bn, T, logT);
+    return pseries_k(ldg(&a[0]), ldg(&a[1]), bn, T, logT);
+}
+
+static __device__ __noinline__ double xrate_dkdt_global(int type, const double *a, const double *x,
+                                                       double k, double T, double logT) {
+    double bn[9];
+    for (int n = 0; n < 9; ++n) bn[n] = ldg(&x[n]);
+    if (type == kJanev) return janev_dkdt(k, ldg(&a[1]), ldg(&a[2]), bn, T, logT);
+    return pseries_dkdt(k, ldg(&a[1]), bn, T);
 }
 
 static __device__ __noinline__ double arr_global(const double *a, double T, double logT) {

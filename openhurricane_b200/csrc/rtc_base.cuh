@@ -27,7 +27,7 @@ constexpr int kMaxSide = 4;
 
 enum RateType : int32_t {
     kArrhenius = 0, kThirdBody = 1, kLindemann = 2, kTroe3 = 3, kTroe4 = 4, kSRI = 5, kPLOG = 6,
-    kLandauTeller = 7
+    kLandauTeller = 7, kJanev = 8, kPowerSeries = 9
 };
 // reversible flags: 1 kr = kf / Kc, 2 kr from explicit reverse Arrhenius parameters
 constexpr int32_t kRevExplicit = 2;
@@ -251,6 +251,54 @@ __device__ __forceinline__ double lt_dkdt(double k, double b, double Ta, double 
     if (fabs(Ta) > kVeryTiny) d += Ta / T;
     if (fabs(B) > kVeryTiny) d -= (B / cbrt(T)) / 3.0;
     if (fabs(C) > kVeryTiny) d -= 2.0 * (C / pow(T, 2.0 / 3.0)) / 3.0;
+    return k * (b + d) / T;
+}
+
+// Janev (JanevRR.cpp:37-88): k = A T^b exp(-Ta/T + sum_{n<9} b_n (ln T)^n),
+// dk/dT = k (b + Ta/T + b_1 + sum_{n>=2} n b_n (ln T)^(n-1)) / T
+__device__ __forceinline__ double janev_k(double A, double b, double Ta, const double *bn, double T,
+                                          double logT) {
+    double e = 0.0;
+    if (fabs(b) > kVeryTiny) e = b * logT;
+    if (fabs(Ta) > kVeryTiny) e -= Ta / T;
+    double lp = 1.0;
+    for (int n = 0; n < 9; ++n) {
+        e += bn[n] * lp;
+        lp *= logT;
+    }
+    return A * exp(e);
+}
+
+__device__ __forceinline__ double janev_dkdt(double k, double b, double Ta, const double *bn,
+                                             double T, double logT) {
+    double d = bn[1], lp = 1.0;
+    for (int n = 2; n < 9; ++n) {
+        lp *= logT;
+        d += n * bn[n] * lp;
+    }
+    return k * (b + Ta / T + d) / T;
+}
+
+// power series (powerSeriesRateRR.cpp:37-74): k = A T^b exp(sum_{n<4} b_n / T^(n+1)),
+// dk/dT = k (b - sum_{n<4} (n+1) b_n / T^(n+1)) / T
+__device__ __forceinline__ double pseries_k(double A, double b, const double *bn, double T,
+                                            double logT) {
+    double e = 0.0;
+    if (fabs(b) > kVeryTiny) e = b * logT;
+    double ti = 1.0 / T, tp = ti;
+    for (int n = 0; n < 4; ++n) {
+        e += bn[n] * tp;
+        tp *= ti;
+    }
+    return A * exp(e);
+}
+
+__device__ __forceinline__ double pseries_dkdt(double k, double b, const double *bn, double T) {
+    double d = 0.0, ti = 1.0 / T, tp = ti;
+    for (int n = 0; n < 4; ++n) {
+        d -= (n + 1) * bn[n] * tp;
+        tp *= ti;
+    }
     return k * (b + d) / T;
 }
 

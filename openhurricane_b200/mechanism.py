@@ -38,8 +38,9 @@ Arrhenius and third-body reactions; non-stoichiometric orders (FORD, RORD).
 pressure-dependent Arrhenius tables (PLOG, logInterpolationRR) on reactions
 without a third body; chemically activated bimolecular reactions (HIGH,
 chemicallyActicatedBimolecularRR) with any fall-off function; Landau-Teller
-rates (LT, LandauTellerRR). The reference's other rate forms (RLT, JAN,
-FIT1, ...) are rejected with NotImplementedError, and so is CHEB, whose
+rates (LT, LandauTellerRR); Janev (JAN, JanevRR) and power-series (FIT1,
+powerSeriesRR) rates. The reference's other forms (RLT, TDEP, ...) are
+rejected with NotImplementedError, and so is CHEB, whose
 reference implementation does not evaluate the Chebyshev fit (see
 parse_chemkin).
 """
@@ -79,6 +80,8 @@ RATE_TROE4 = 4
 RATE_SRI = 5
 RATE_PLOG = 6
 RATE_LANDAU_TELLER = 7
+RATE_JANEV = 8
+RATE_POWER_SERIES = 9
 
 # reversibility codes
 IRREVERSIBLE = 0
@@ -93,7 +96,7 @@ UNITS_E = {"CAL": "CAL", "CAL/MOLE": "CAL", "EVOL": "EVOL", "EVOLTS": "EVOL", "J
            "KELVINS": "KELV", "KJOU": "KJOU", "KJOULES/MOLE": "KJOU"}
 ELECTRON_VOLT = 1.6021766208e-19    # J (physicalConstant.hpp:59,114)
 # auxiliary keywords of the reference's reader that this reader does not take
-_UNSUPPORTED_AUX = {"CHEB", "PCHEB", "TCHEB", "RLT", "JAN", "FIT1", "TDEP",
+_UNSUPPORTED_AUX = {"CHEB", "PCHEB", "TCHEB", "RLT", "TDEP",
                     "XSMI", "MOME", "EXCI", "COLLEFF"}
 
 
@@ -119,6 +122,8 @@ class ParsedReaction:
     high: Optional[Tuple[float, float, float]] = None   # HIGH A, b, E (chemically activated)
     lt: Optional[Tuple[float, float]] = None             # Landau-Teller B, C
     named_third: Optional[int] = None                    # species of a (+X) third body
+    janev: Optional[List[float]] = None                  # JAN b_0..b_8
+    fit1: Optional[List[float]] = None                   # FIT1 b_0..b_3
 
 
 @dataclasses.dataclass
@@ -160,6 +165,7 @@ class MechTables:
     plog_arr: Optional[np.ndarray] = None  # [n, 3] A, beta, Ta
     activated: Optional[np.ndarray] = None  # [nrc] int32 1: chemically activated (HIGH)
     lt: Optional[np.ndarray] = None        # [nrc, 2] Landau-Teller B, C
+    xcoef: Optional[np.ndarray] = None     # [nrc, 9] Janev b_0..b_8 / power-series b_0..b_3
 
     @property
     def nsp(self) -> int:
@@ -339,6 +345,18 @@ def parse_chemkin(che_text: str, species_names: Optional[List[str]] = None):
                 if cur.kind != "falloff":
                     raise ValueError("HIGH needs a pressure-dependent (+M) reaction")
                 cur.high = (_read_real(v[0]), _read_real(v[1]), _read_real(v[2]))
+            elif up in ("JAN", "FIT1"):
+                # chemkinFileRead.cpp:479-529: 9 Janev or 4 power-series coefficients
+                # on a reaction without a third body
+                if cur.kind != "arrhenius":
+                    raise ValueError(f"{up} cannot be used on a third-body or fall-off reaction")
+                want = 9 if up == "JAN" else 4
+                if len(v) != want:
+                    raise ValueError(f"{up} takes {want} coefficients")
+                if up == "JAN":
+                    cur.janev = [_read_real(x) for x in v]
+                else:
+                    cur.fit1 = [_read_real(x) for x in v]
             elif up == "LT":
                 # chemkinFileRead.cpp:413-440: not on a pressure-dependent reaction
                 if cur.kind != "arrhenius":
@@ -505,6 +523,7 @@ def compile_mechanism(che_path: str, thermo_path: Optional[str] = None,
     plog_rows = []
     activated = np.zeros(nrc, np.int32)
     lt = np.zeros((nrc, 2))
+    xcoef = np.zeros((nrc, 9))
     for r, rx in enumerate(reactions):
         if len(rx.fwd) > MAX_SIDE or len(rx.bwd) > MAX_SIDE:
             raise ValueError("too many species on one side")
@@ -531,6 +550,19 @@ def compile_mechanism(che_path: str, thermo_path: Optional[str] = None,
             rate_type[r] = RATE_PLOG
             arr[r] = (rx.A * Afac, rx.b, rx.E / Efac)
             plog_rows.append((r, [(pa * PATM, A_ * Afac, b_, E_ / Efac) for pa, A_, b_, E_ in ent]))
+        elif rx.janev is not None or rx.fit1 is not None:
+            if rx.rev is not None:
+                raise ValueError("REV cannot be used with a Janev or power-series rate")
+            # JanevRR: A, beta, Ta from the main line; powerSeriesRR: A and beta
+            # only (chemkinFileRead.cpp:1531-1534, 1575-1577)
+            if rx.janev is not None:
+                rate_type[r] = RATE_JANEV
+                arr[r] = (rx.A * Afac, rx.b, rx.E / Efac)
+                xcoef[r] = rx.janev
+            else:
+                rate_type[r] = RATE_POWER_SERIES
+                arr[r] = (rx.A * Afac, rx.b, 0.0)
+                xcoef[r, :4] = rx.fit1
         elif rx.lt is not None:
             if rx.rev is not None:
                 # the reference needs RLT with REV here, which this reader does not take
@@ -625,7 +657,7 @@ def compile_mechanism(che_path: str, thermo_path: Optional[str] = None,
                       eff, nf, nb, fidx, bidx, fnu, bnu, ford, bord, sum_stoi,
                       geom, eps, sig, dip, pol, zr, sri=sri, arr_rev=arr_rev,
                       plog_ptr=plog_ptr, plog_p=plog_p, plog_arr=plog_arr,
-                      activated=activated, lt=lt)
+                      activated=activated, lt=lt, xcoef=xcoef)
 
 
 def element_matrix_mass(m: MechTables) -> np.ndarray:

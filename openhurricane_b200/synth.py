@@ -72,6 +72,8 @@ class Reaction:
     #                                                  # PLOG p [atm], A, b, Ea (cal/mol)
     activated: bool = False     # chemically activated: main line = low, HIGH = (A, b, Ea)
     lt: Optional[Tuple[float, float]] = None           # Landau-Teller B, C
+    janev: Optional[Tuple[float, ...]] = None          # JAN b_0..b_8
+    fit1: Optional[Tuple[float, ...]] = None           # FIT1 b_0..b_3
 
 
 @dataclasses.dataclass
@@ -373,6 +375,23 @@ def extended_mechanism(seed: int = 20241117) -> Mechanism:
     return m
 
 
+def fitted_rates_mechanism(seed: int = 20240901) -> Mechanism:
+    """The small mechanism with one reaction on a Janev rate (JAN, nine
+    coefficients of powers of ln T) and one on a power-series rate (FIT1,
+    four coefficients of powers of 1/T), small enough to keep the rates within
+    a decade or so of the drawn Arrhenius ones."""
+    m = small_mechanism(seed)
+    rng = np.random.default_rng(seed + 7)
+    plain = [r for r in m.reactions if r.kind == "plain"]
+    plain[0].janev = tuple(float(np.round(rng.uniform(-1.0, 1.0) * 0.3 / 8.0 ** n, 10))
+                           for n in range(9))
+    plain[1].fit1 = (float(np.round(rng.uniform(-300.0, 300.0), 4)),
+                     float(np.round(rng.uniform(-1e5, 1e5), 2)),
+                     float(np.round(rng.uniform(-1e7, 1e7), 1)),
+                     float(np.round(rng.uniform(-1e9, 1e9), 1)))
+    return m
+
+
 def small_mechanism(seed: int = 20240901) -> Mechanism:
     """9 species / 21 reversible Arrhenius reactions, 3 third-body, 1 Troe."""
     return make_mechanism(9, 21, 3, 1, seed)
@@ -478,6 +497,10 @@ def write_chemkin(mech: Mechanism, out_dir: str, stem: str = "mech") -> Tuple[st
             lines.append(f"   PLOG / {pa:g}  {A(Ap, fo):.6E}  {bp:.6f}  {E(Ep):.4f} /")
         if r.lt is not None:
             lines.append(f"   LT / {r.lt[0]:g}  {r.lt[1]:g} /")
+        if r.janev is not None:
+            lines.append("   JAN / " + "  ".join(f"{x:.10g}" for x in r.janev) + " /")
+        if r.fit1 is not None:
+            lines.append("   FIT1 / " + "  ".join(f"{x:.10g}" for x in r.fit1) + " /")
     lines += ["END", ""]
     with open(che, "w") as f:
         f.write("\n".join(lines))

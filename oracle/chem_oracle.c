@@ -15,7 +15,8 @@
  *                 fallOffFunctions.cpp:81-157 (Troe), :54-79 (SRI), fallOffFunctions.hpp
  *                 (Lindemann); reversibleReactionWithRevPars.hpp:68-122 (Chemkin REV);
  *                 logInterpolationRR.cpp:78-226 (PLOG), LandauTellerRR.cpp:37-99 (LT),
- *                 chemicallyActicatedBimolecularRR.cpp:36-96 (HIGH)
+ *                 chemicallyActicatedBimolecularRR.cpp:36-96 (HIGH), JanevRR.cpp:37-88 (JAN),
+ *                 powerSeriesRateRR.cpp:37-74 (FIT1)
  *   reactions     reactionTypes/src/reactionTypes.cpp:178-352 (Kp, DKpDT, Kc, DKcDT, q),
  *                 :354-445 (DqDci), :843-876 (DqDT); reversibleReactions.hpp:62-127;
  *                 irreversibleReactions.hpp; reactionList.hpp:83-86 (updateG0)
@@ -401,6 +402,57 @@ static double ltDkDT(const hc_mech_desc *m, int r, double T) {
     return lta * (a[1] + deriv) / T;
 }
 
+/* Janev (JanevRR.cpp:37-88) and power series (powerSeriesRateRR.cpp:37-74) */
+static double janevK(const hc_mech_desc *m, int r, double T) {
+    const double *a = &m->arr[3 * r], *b = &m->xcoef[9 * r];
+    double lta = a[0];
+    if (fabs(a[1]) > VERY_TINY) lta *= pow(T, a[1]);
+    double expArg = 0.0;
+    if (fabs(a[2]) > VERY_TINY) expArg -= a[2] / T;
+    const double lnT = log(T);
+    for (int n = 0; n < 9; n++) expArg += b[n] * pow(lnT, n);
+    lta *= exp(expArg);
+    return lta;
+}
+
+static double janevDkDT(const hc_mech_desc *m, int r, double T) {
+    const double *a = &m->arr[3 * r], *b = &m->xcoef[9 * r];
+    double lta = a[0];
+    if (fabs(a[1]) > VERY_TINY) lta *= pow(T, a[1]);
+    double expArg = 0;
+    if (fabs(a[2]) > VERY_TINY) expArg -= a[2] / T;
+    const double lnT = log(T);
+    for (int n = 0; n < 9; n++) expArg += b[n] * pow(lnT, n);
+    double deriv = b[1];
+    for (int n = 2; n < 9; n++) deriv += n * b[n] * pow(lnT, n - 1);
+    lta *= exp(expArg);
+    return lta * (a[1] + a[2] / T + deriv) / T;
+}
+
+static double pseriesK(const hc_mech_desc *m, int r, double T) {
+    const double *a = &m->arr[3 * r], *b = &m->xcoef[9 * r];
+    double lta = a[0];
+    if (fabs(a[1]) > VERY_TINY) lta *= pow(T, a[1]);
+    double expArg = 0.0;
+    for (int n = 0; n < 4; n++) expArg += b[n] / pow(T, n + 1);
+    lta *= exp(expArg);
+    return lta;
+}
+
+static double pseriesDkDT(const hc_mech_desc *m, int r, double T) {
+    const double *a = &m->arr[3 * r], *b = &m->xcoef[9 * r];
+    double lta = a[0];
+    if (fabs(a[1]) > VERY_TINY) lta *= pow(T, a[1]);
+    double expArg = 0, deriv = 0;
+    for (int n = 0; n < 4; n++) {
+        const double cT = b[n] / pow(T, n + 1);
+        expArg += cT;
+        deriv -= (n + 1) * cT;
+    }
+    lta *= exp(expArg);
+    return lta * (a[1] + deriv) / T;
+}
+
 /* chemically activated bimolecular (Chemkin HIGH,
    chemicallyActicatedBimolecularRR.cpp:36-96): k = k0 F / (1 + Pr) */
 static int activated(const hc_mech_desc *m, int r) { return m->activated && m->activated[r]; }
@@ -411,6 +463,8 @@ static double rateK(const hc_mech_desc *m, int r, double p, double T, const doub
     if (t == HC_RATE_ARRHENIUS) return arrK(a, T);
     if (t == HC_RATE_PLOG) return plogK(m, r, p, T);
     if (t == HC_RATE_LANDAU_TELLER) return ltK(m, r, T);
+    if (t == HC_RATE_JANEV) return janevK(m, r, T);
+    if (t == HC_RATE_POWER_SERIES) return pseriesK(m, r, T);
     if (t == HC_RATE_THIRD_BODY) {
         const double M = thirdM(m, r, c);
         return (M * arrK(a, T));
@@ -429,6 +483,8 @@ static double rateDkDT(const hc_mech_desc *m, int r, double kj, double p, double
     if (t == HC_RATE_ARRHENIUS || t == HC_RATE_THIRD_BODY) return arrDkDT(a, kj, T);
     if (t == HC_RATE_PLOG) return plogDkDT(m, r, kj, p, T);
     if (t == HC_RATE_LANDAU_TELLER) return ltDkDT(m, r, T);
+    if (t == HC_RATE_JANEV) return janevDkDT(m, r, T);
+    if (t == HC_RATE_POWER_SERIES) return pseriesDkDT(m, r, T);
     const double k0 = arrK(&m->arr0[3 * r], T);
     const double kinf = arrK(a, T);
     const double Pr = k0 / notZeroD(kinf) * thirdM(m, r, c);
@@ -465,9 +521,7 @@ static void gamDGamDCi(const hc_mech_desc *m, int r, double T, const double *c, 
 
 static double gamDGamDT(const hc_mech_desc *m, int r, double T, const double *c) {
     const int t = m->rate_type[r];
-    if (t == HC_RATE_ARRHENIUS || t == HC_RATE_THIRD_BODY || t == HC_RATE_PLOG ||
-        t == HC_RATE_LANDAU_TELLER)
-        return 0.0;
+    if (t == HC_RATE_ARRHENIUS || t == HC_RATE_THIRD_BODY || t >= HC_RATE_PLOG) return 0.0;
     const double M = thirdM(m, r, c);
     if (M > TINY) {
         const double *a0 = &m->arr0[3 * r], *a = &m->arr[3 * r];
@@ -626,8 +680,7 @@ static void DqDci(const mech_ctx *x, int r, double kf, double kr, double qfr, do
         for (int j = 0; j < nb; ++j) J[bi[j] * n + si] -= bnu[j] * d;
     }
     const int t = m->rate_type[r];
-    if (t != HC_RATE_ARRHENIUS && t != HC_RATE_PLOG &&
-        t != HC_RATE_LANDAU_TELLER) {   /* hasThirdBodyTerms() */
+    if (t != HC_RATE_ARRHENIUS && t < HC_RATE_PLOG) {   /* hasThirdBodyTerms() */
         double *g = scratch;
         gamDGamDCi(m, r, T, c, g);
         for (int i = 0; i < m->nsp; ++i) {

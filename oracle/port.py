@@ -65,7 +65,7 @@ class HcMechDesc(C.Structure):
         ("geom", C.c_void_p), ("eps_k", C.c_void_p), ("sigma", C.c_void_p),
         ("sri", C.c_void_p), ("arr_rev", C.c_void_p),
         ("plog_ptr", C.c_void_p), ("plog_p", C.c_void_p), ("plog_arr", C.c_void_p),
-        ("activated", C.c_void_p), ("lt", C.c_void_p),
+        ("activated", C.c_void_p), ("lt", C.c_void_p), ("xcoef", C.c_void_p),
     ]
 
 
@@ -111,7 +111,8 @@ class MechDesc:
             sigma=f64(t.sigma), sri=f64(_sri(t)), arr_rev=f64(_arr_rev(t)),
             plog_ptr=i32(_plog(t)[0]), plog_p=f64(_plog(t)[1]), plog_arr=f64(_plog(t)[2]),
             activated=i32(_opt(t, "activated", (t.nrc,), np.int32)),
-            lt=f64(_opt(t, "lt", (t.nrc, 2), np.float64)))
+            lt=f64(_opt(t, "lt", (t.nrc, 2), np.float64)),
+            xcoef=f64(_opt(t, "xcoef", (t.nrc, 9), np.float64)))
         d = HcMechDesc()
         d.nsp, d.nrc = t.nsp, t.nrc
         for k, a in self.arrays.items():

@@ -21,7 +21,7 @@ def mech_dir(tmp_path_factory):
 def _make(name, mech_dir):
     from openhurricane_b200 import synth, mechanism
     m = {"small": synth.small_mechanism, "large": synth.large_mechanism,
-         "ext": synth.extended_mechanism}[name]()
+         "ext": synth.extended_mechanism, "fitted": synth.fitted_rates_mechanism}[name]()
     d = os.path.join(mech_dir, name)
     che, th, tr = synth.write_chemkin(m, d)
     tables = mechanism.compile_mechanism(che, th, tr)
@@ -42,3 +42,9 @@ def large(mech_dir):
 def ext(mech_dir):
     """The small mechanism's species with SRI, REV, FORD / RORD and unit keywords."""
     return _make("ext", mech_dir)
+
+
+@pytest.fixture(scope="session")
+def fitted(mech_dir):
+    """The small mechanism with one Janev (JAN) and one power-series (FIT1) rate."""
+    return _make("fitted", mech_dir)

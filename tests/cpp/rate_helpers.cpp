@@ -4,6 +4,8 @@
 //   "S a b c d e T Pr F DPrDT"  -> sri_F, sri_dfdt, sri_dfdci_factor
 //   "P n p T  p_1 A_1 b_1 Ta_1 ... p_n A_n b_n Ta_n"  -> plog_k, plog_dkdt
 //   "L A b Ta B C T"  -> lt_k, lt_dkdt
+//   "J A b Ta b_0 .. b_8 T"  -> janev_k, janev_dkdt
+//   "F A b b_0 .. b_3 T"  -> pseries_k, pseries_dkdt
 #include <cmath>
 #include <cstdio>
 
@@ -37,6 +39,22 @@ int main() {
             if (std::scanf("%lf %lf %lf %lf %lf %lf", &A, &b, &Ta, &B, &C, &T) != 6) return 1;
             const double k = hc::lt_k(A, b, Ta, B, C, T, std::log(T));
             std::printf("%.17g %.17g\n", k, hc::lt_dkdt(k, b, Ta, B, C, T));
+        } else if (kind[0] == 'J' || kind[0] == 'F') {
+            const int nb = kind[0] == 'J' ? 9 : 4;
+            double A, b, Ta = 0.0, bn[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, T;
+            if (std::scanf("%lf %lf", &A, &b) != 2) return 1;
+            if (kind[0] == 'J' && std::scanf("%lf", &Ta) != 1) return 1;
+            for (int i = 0; i < nb; ++i)
+                if (std::scanf("%lf", &bn[i]) != 1) return 1;
+            if (std::scanf("%lf", &T) != 1) return 1;
+            const double lT = std::log(T);
+            if (kind[0] == 'J') {
+                const double k = hc::janev_k(A, b, Ta, bn, T, lT);
+                std::printf("%.17g %.17g\n", k, hc::janev_dkdt(k, b, Ta, bn, T, lT));
+            } else {
+                const double k = hc::pseries_k(A, b, bn, T, lT);
+                std::printf("%.17g %.17g\n", k, hc::pseries_dkdt(k, b, bn, T));
+            }
         } else {
             return 1;
         }

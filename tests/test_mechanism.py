@@ -193,3 +193,26 @@ def test_thermo_and_transport_sections_in_the_mechanism_file(small, tmp_path):
     b = M.compile_mechanism(str(one))
     for k in ("W", "nasa", "Trange", "arr", "arr0", "troe", "eff", "geom", "eps_k", "sigma"):
         assert np.array_equal(getattr(a, k), getattr(b, k)), k
+
+
+def test_janev_and_power_series_tables(fitted):
+    """JAN keeps A, beta and Ta of the main line and 9 coefficients; FIT1 keeps
+    A and beta (its E is not used) and 4 coefficients in the first columns."""
+    t = fitted["tables"]
+    m = fitted["mech"]
+    rx = m.reactions
+    j = next(i for i, r in enumerate(rx) if r.janev is not None)
+    f = next(i for i, r in enumerate(rx) if r.fit1 is not None)
+    assert t.rate_type[j] == M.RATE_JANEV and t.rate_type[f] == M.RATE_POWER_SERIES
+    assert np.array_equal(t.xcoef[j], np.array(rx[j].janev))
+    assert np.array_equal(t.xcoef[f, :4], np.array(rx[f].fit1))
+    assert not t.xcoef[f, 4:].any()
+    assert t.arr[f, 2] == 0.0 and t.arr[j, 2] > 0.0
+    others = [i for i in range(len(rx)) if i not in (j, f)]
+    assert not t.xcoef[others].any()
+    import pytest
+    with pytest.raises(ValueError, match="JAN"):
+        M.parse_chemkin(_che("H2+O2(+M)=2HO(+M) 1.0E13 0.0 1000.0\n LOW / 1.0E16 0.0 0.0 /\n"
+                             " JAN / 1 2 3 4 5 6 7 8 9 /"))
+    with pytest.raises(ValueError, match="FIT1 takes 4"):
+        M.parse_chemkin(_che("H2+O2=2HO 1.0E13 0.0 1000.0\n FIT1 / 1 2 3 /"))

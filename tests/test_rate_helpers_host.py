@@ -220,3 +220,37 @@ def test_landau_teller_helpers_match_the_reference(exe):
         k, d = _lt_ref(*c)
         assert abs(g[0] - k) <= 1e-13 * abs(k), c
         assert abs(g[1] - d) <= 1e-12 * max(abs(d), 1e-300) + 1e-14 * abs(k) / c[-1], c
+
+
+def test_janev_and_power_series_helpers_match_the_reference(exe):
+    """JanevRR (JanevRR.cpp:37-88) and powerSeriesRR (powerSeriesRateRR.cpp:37-74)."""
+    rng = np.random.default_rng(10)
+    jan, fit = [], []
+    for _ in range(100):
+        A, b, Ta = float(10.0 ** rng.uniform(6, 14)), float(rng.uniform(-1, 2)), float(rng.uniform(0, 3e4))
+        bn = [float(rng.uniform(-1, 1) * 0.3 / 8.0 ** n) for n in range(9)]
+        T = float(rng.uniform(300, 3000))
+        jan.append((A, b, Ta, bn, T))
+        fn = [float(rng.uniform(-300, 300)), float(rng.uniform(-1e5, 1e5)),
+              float(rng.uniform(-1e7, 1e7)), float(rng.uniform(-1e9, 1e9))]
+        fit.append((A, b, fn, T))
+    txt = "".join(f"J {A!r} {b!r} {Ta!r} " + " ".join(repr(x) for x in bn) + f" {T!r}\n"
+                  for A, b, Ta, bn, T in jan)
+    txt += "".join(f"F {A!r} {b!r} " + " ".join(repr(x) for x in fn) + f" {T!r}\n"
+                   for A, b, fn, T in fit)
+    out = subprocess.run([exe], input=txt, capture_output=True, text=True, check=True).stdout
+    got = np.array([[float(x) for x in l.split()] for l in out.strip().splitlines()])
+    for (A, b, Ta, bn, T), g in zip(jan, got[:100]):
+        lnT = math.log(T)
+        e = -Ta / T + sum(bn[n] * math.pow(lnT, n) for n in range(9))
+        k = A * math.pow(T, b) * math.exp(e)
+        d = bn[1] + sum(n * bn[n] * math.pow(lnT, n - 1) for n in range(2, 9))
+        dk = k * (b + Ta / T + d) / T
+        assert abs(g[0] - k) <= 1e-13 * abs(k)
+        assert abs(g[1] - dk) <= 1e-12 * abs(dk) + 1e-14 * abs(k) / T
+    for (A, b, fn, T), g in zip(fit, got[100:]):
+        e = sum(fn[n] / math.pow(T, n + 1) for n in range(4))
+        k = A * math.pow(T, b) * math.exp(e)
+        dk = k * (b - sum((n + 1) * fn[n] / math.pow(T, n + 1) for n in range(4))) / T
+        assert abs(g[0] - k) <= 1e-13 * abs(k)
+        assert abs(g[1] - dk) <= 1e-12 * abs(dk) + 1e-14 * abs(k) / T

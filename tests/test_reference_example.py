@@ -117,3 +117,30 @@ def test_named_third_body_falloff_matches_the_reference(small, tmp_path):
                        opts=port.default_opts(atol=1e-15))
     for k in ("T", "Y", "rho", "c", "subdt"):
         assert np.array_equal(o[k], ref[k]), k
+
+
+def test_fitted_rates_match_the_reference(fitted, tmp_path):
+    """Janev (JAN) and power-series (FIT1) rates: reader and oracle against the
+    reference build, by integration and known answers."""
+    from oracle import port, refrun
+    if not refrun.available():
+        pytest.skip("reference binary not built (make -f oracle/Makefile.ref)")
+    t = fitted["tables"]
+    assert sorted(set(t.rate_type) & {8, 9}) == [8, 9]
+    case = str(tmp_path / "case.cont")
+    refrun.write_case(case, *fitted["files"], {"atol": 1e-15})
+    from openhurricane_b200 import synth
+    c = synth.dirichlet_cells(t.nsp, 12, seed=41)
+    rho = synth.mixture_density(t.W, c)
+    r = refrun.integrate(case, c.T, c.p, rho, 1e-6, 1e-6, c.Y, procs=4, workdir=str(tmp_path))
+    md = port.MechDesc(t)
+    o = port.integrate(md, c.T, c.p, rho, c.Y, 1e-6, opts=port.default_opts(atol=1e-15))
+    for k in ("T", "Y", "rho", "c", "subdt"):
+        assert np.array_equal(o[k], r[k]), k
+    rng = np.random.default_rng(3)
+    T = rng.uniform(800.0, 3000.0, 6)
+    p = rng.uniform(1.0, 5.0, 6) * 101325.0
+    cc = rng.dirichlet(np.full(t.nsp, 0.5), 6).T.copy() * 0.01
+    k = refrun.kat(case, p, T, cc, workdir=str(tmp_path))
+    f, J = port.rhs_jac(md, cc, T, p)
+    assert np.array_equal(f, k["dydt"]) and np.array_equal(J, k["J"])

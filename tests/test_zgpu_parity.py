@@ -469,3 +469,38 @@ def test_temperature_from_energy_vs_reference_golden(name, request):
                                         d(g0[name + "_tea_rho"]), d(g0[name + "_tea_T0"]))
     assert np.array_equal(flag.cpu().numpy(), g0[name + "_tea_flag"])
     assert np.abs(T.cpu().numpy() - g0[name + "_tea_T"]).max() < 1e-6
+
+
+@pytest.mark.parametrize("kernel", [0, 2])
+def test_fitted_rates_parity_vs_oracle(fitted, kernel):
+    """Janev (JAN) and power-series (FIT1) rates through the cell-group kernel
+    against the oracle (pinned to the reference); over 1e-7 s these cells are
+    well conditioned (one-ulp input changes move T by 6e-10 in the oracle) and
+    take at most 39503 Newton iterations each."""
+    t = fitted["tables"]
+    T, p, rho, Y = _cells(t, 96, seed=23)
+    m = _mech(t)
+    m.set_tuning(kernel, 64)
+    g = _gpu_integrate(m, T, p, rho, Y, 1e-7, max_newton_total=1000000, **PARITY)
+    o = _oracle(t, T, p, rho, Y, 1e-7, key="fitted96", **PARITY)
+    assert np.array_equal(g["status"] & 12, np.zeros_like(g["status"]))
+    _assert_close(g, o, f"fitted rates, kernel {kernel}")
+
+
+def test_fitted_rates_rhs_jacobian_vs_oracle(fitted):
+    from oracle import port
+    dev = _cuda()
+    t = fitted["tables"]
+    rng = np.random.default_rng(3)
+    n = 16
+    T = rng.uniform(800.0, 3000.0, n)
+    p = rng.uniform(1.0, 5.0, n) * 101325.0
+    c = rng.dirichlet(np.full(t.nsp, 0.5), n).T.copy() * 0.01
+    m = _mech(t)
+    d = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+    dydt, J = m.rhs_jacobian(d(c), d(T), d(p))
+    ref_f, ref_J = port.rhs_jac(port.MechDesc(t), c, T, p)
+    sf = np.abs(ref_f).max(axis=1, keepdims=True) + 1e-300
+    assert (np.abs(dydt.cpu().numpy() - ref_f) / sf).max() < 1e-11
+    sJ = np.abs(ref_J).max(axis=(1, 2), keepdims=True) + 1e-300
+    assert (np.abs(J.cpu().numpy() - ref_J) / sJ).max() < 1e-11
