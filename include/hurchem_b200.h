@@ -66,8 +66,9 @@ extern "C" {
 #define HC_IRREVERSIBLE 0
 #define HC_REVERSIBLE 1         /* kr = kf / Kc (reversibleReactions) */
 #define HC_REVERSIBLE_REV 2     /* kr from explicit reverse Arrhenius parameters, Chemkin REV
-                                   (reversibleReactionWithRevPars); Arrhenius and third-body
-                                   rate laws only, as in the reference */
+                                   (reversibleReactionWithRevPars); Arrhenius, third-body and
+                                   Landau-Teller rate laws (the last with the reverse B, C of
+                                   Chemkin RLT in xcoef), as in the reference */
 
 #define HC_MAX_SIDE 4
 
@@ -119,7 +120,9 @@ typedef struct hc_mech_desc {
     const int32_t *activated; /* [nrc] */
     const double *lt;        /* [nrc*2] Landau-Teller B, C (HC_RATE_LANDAU_TELLER); NULL: none */
     const double *xcoef;     /* [nrc*9] Janev b_0..b_8 or power-series b_0..b_3 (then zeros);
-                                NULL: none */
+                                for a Landau-Teller reaction with HC_REVERSIBLE_REV, the
+                                reverse rate's B, C (Chemkin RLT): kr is then the
+                                Landau-Teller law on arr_rev and these. NULL: none */
 } hc_mech_desc;
 
 /*

@@ -302,8 +302,9 @@ static int check_desc(const hc_mech_desc *d) {
             return fail(HC_E_INVALID, "chemically activated reaction without a fall-off form");
         if (d->rate_type[r] == HC_RATE_LANDAU_TELLER) {
             if (!d->lt) return fail(HC_E_INVALID, "Landau-Teller reaction without its B, C");
-            if (d->reversible[r] == HC_REVERSIBLE_REV)
-                return fail(HC_E_INVALID, "explicit reverse parameters on a Landau-Teller reaction");
+            if (d->reversible[r] == HC_REVERSIBLE_REV && !d->xcoef)
+                return fail(HC_E_INVALID,
+                            "Landau-Teller reaction with REV parameters but no reverse B, C");
         }
         if (d->reversible[r] < HC_IRREVERSIBLE || d->reversible[r] > HC_REVERSIBLE_REV)
             return fail(HC_E_INVALID, "unknown reversibility code");

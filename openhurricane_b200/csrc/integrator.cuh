@@ -233,8 +233,10 @@ struct CellCtx {
         const bool rev = rev_kind != 0;
         if (X && rev_kind == kRevExplicit) {
             // reversibleReactionWithRevPars::kr (reversibleReactionWithRevPars.hpp:68-76):
-            // the reverse rate law of the same kind, M times it for third-body
-            kr = arr_global(&m.arr_rev[3 * r], T, logT);
+            // the reverse rate law of the same kind, M times it for third-body;
+            // a Landau-Teller reaction's reverse B, C (Chemkin RLT) sit in xcoef
+            if (type == kLandauTeller) kr = lt_k_global(&m.arr_rev[3 * r], &m.xcoef[9 * r], T, logT);
+            else kr = arr_global(&m.arr_rev[3 * r], T, logT);
             if (type == kThirdBody) kr = M * kr;
         } else if (rev) {
             const double *sg = s;
@@ -320,7 +322,9 @@ struct CellCtx {
             dkfdT = (Pr / (1.0 + Pr)) * F * (kinf * invT * (b + Ta * invT));
         }
         double dkrdT = 0.0;
-        if (X && rev_kind == kRevExplicit)
+        if (X && rev_kind == kRevExplicit && type == kLandauTeller)
+            dkrdT = lt_dkdt_global(&m.arr_rev[3 * r], &m.xcoef[9 * r], kr, T);
+        else if (X && rev_kind == kRevExplicit)
             dkrdT = kr * invT * (ldg(&m.arr_rev[3 * r + 1]) + ldg(&m.arr_rev[3 * r + 2]) * invT);
         else if (rev) dkrdT = (dkfdT - kr * DKcDT) / hmax(Kc, kVeryTiny);
 #pragma unroll

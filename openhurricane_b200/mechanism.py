@@ -96,7 +96,7 @@ UNITS_E = {"CAL": "CAL", "CAL/MOLE": "CAL", "EVOL": "EVOL", "EVOLTS": "EVOL", "J
            "KELVINS": "KELV", "KJOU": "KJOU", "KJOULES/MOLE": "KJOU"}
 ELECTRON_VOLT = 1.6021766208e-19    # J (physicalConstant.hpp:59,114)
 # auxiliary keywords of the reference's reader that this reader does not take
-_UNSUPPORTED_AUX = {"CHEB", "PCHEB", "TCHEB", "RLT", "TDEP",
+_UNSUPPORTED_AUX = {"CHEB", "PCHEB", "TCHEB", "TDEP",
                     "XSMI", "MOME", "EXCI", "COLLEFF"}
 
 
@@ -121,6 +121,7 @@ class ParsedReaction:
     plog: Optional[List[Tuple[float, float, float, float]]] = None   # (p atm, A, b, E) as read
     high: Optional[Tuple[float, float, float]] = None   # HIGH A, b, E (chemically activated)
     lt: Optional[Tuple[float, float]] = None             # Landau-Teller B, C
+    rlt: Optional[Tuple[float, float]] = None            # reverse Landau-Teller B, C (RLT)
     named_third: Optional[int] = None                    # species of a (+X) third body
     janev: Optional[List[float]] = None                  # JAN b_0..b_8
     fit1: Optional[List[float]] = None                   # FIT1 b_0..b_3
@@ -362,6 +363,14 @@ def parse_chemkin(che_text: str, species_names: Optional[List[str]] = None):
                 if cur.kind != "arrhenius":
                     raise ValueError("LT cannot be used on a third-body or fall-off reaction")
                 cur.lt = (_read_real(v[0]), _read_real(v[1]))
+            elif up == "RLT":
+                # chemkinFileRead.cpp:441-478: the reverse rate of a REV reaction in
+                # the Landau-Teller form, with REV's A, beta, Ta
+                if cur.kind != "arrhenius":
+                    raise ValueError("RLT cannot be used on a third-body or fall-off reaction")
+                if cur.rev is None:
+                    raise ValueError("The keyword RLT must follow the explicit REV parameters")
+                cur.rlt = (_read_real(v[0]), _read_real(v[1]))
             elif up == "REV":
                 cur.rev = (_read_real(v[0]), _read_real(v[1]), _read_real(v[2]))
             elif up in ("FORD", "RORD"):
@@ -550,6 +559,10 @@ def compile_mechanism(che_path: str, thermo_path: Optional[str] = None,
             rate_type[r] = RATE_PLOG
             arr[r] = (rx.A * Afac, rx.b, rx.E / Efac)
             plog_rows.append((r, [(pa * PATM, A_ * Afac, b_, E_ / Efac) for pa, A_, b_, E_ in ent]))
+        elif rx.rlt is not None and rx.lt is None:
+            # the rate type turns Landau-Teller without its LT parameters: the
+            # reference aborts there (chemkinFileRead.cpp:1503, a failed cast)
+            raise ValueError("RLT on a reaction without LT")
         elif rx.janev is not None or rx.fit1 is not None:
             if rx.rev is not None:
                 raise ValueError("REV cannot be used with a Janev or power-series rate")
@@ -564,12 +577,16 @@ def compile_mechanism(che_path: str, thermo_path: Optional[str] = None,
                 arr[r] = (rx.A * Afac, rx.b, 0.0)
                 xcoef[r, :4] = rx.fit1
         elif rx.lt is not None:
-            if rx.rev is not None:
-                # the reference needs RLT with REV here, which this reader does not take
-                raise ValueError("REV on a Landau-Teller reaction")
+            if rx.rev is not None and rx.rlt is None:
+                # the reference builds no reverse rate for REV without RLT here
+                # (chemkinFileRead.cpp:1507-1512 reads a null one)
+                raise ValueError("REV on a Landau-Teller reaction needs RLT")
             rate_type[r] = RATE_LANDAU_TELLER
             arr[r] = (rx.A * Afac, rx.b, rx.E / Efac)
             lt[r] = rx.lt
+            if rx.rlt is not None:
+                # reverse Landau-Teller B, C beside the REV parameters
+                xcoef[r, :2] = rx.rlt
         elif rx.kind == "arrhenius":
             rate_type[r] = RATE_ARRHENIUS
             arr[r] = (rx.A * Afac, rx.b, rx.E / Efac)

@@ -72,6 +72,7 @@ class Reaction:
     #                                                  # PLOG p [atm], A, b, Ea (cal/mol)
     activated: bool = False     # chemically activated: main line = low, HIGH = (A, b, Ea)
     lt: Optional[Tuple[float, float]] = None           # Landau-Teller B, C
+    rlt: Optional[Tuple[float, float]] = None          # reverse Landau-Teller B, C (with rev)
     janev: Optional[Tuple[float, ...]] = None          # JAN b_0..b_8
     fit1: Optional[Tuple[float, ...]] = None           # FIT1 b_0..b_3
 
@@ -379,7 +380,8 @@ def fitted_rates_mechanism(seed: int = 20240901) -> Mechanism:
     """The small mechanism with one reaction on a Janev rate (JAN, nine
     coefficients of powers of ln T) and one on a power-series rate (FIT1,
     four coefficients of powers of 1/T), small enough to keep the rates within
-    a decade or so of the drawn Arrhenius ones."""
+    a decade or so of the drawn Arrhenius ones, and one Landau-Teller reaction
+    with explicit reverse parameters in the Landau-Teller form (LT, REV, RLT)."""
     m = small_mechanism(seed)
     rng = np.random.default_rng(seed + 7)
     plain = [r for r in m.reactions if r.kind == "plain"]
@@ -389,6 +391,13 @@ def fitted_rates_mechanism(seed: int = 20240901) -> Mechanism:
                      float(np.round(rng.uniform(-1e5, 1e5), 2)),
                      float(np.round(rng.uniform(-1e7, 1e7), 1)),
                      float(np.round(rng.uniform(-1e9, 1e9), 1)))
+    plain[2].lt = (float(np.round(rng.uniform(-20.0, 20.0), 4)),
+                   float(np.round(rng.uniform(-50.0, 50.0), 4)))
+    plain[2].rev = (float(10.0 ** np.round(rng.uniform(9.0, 13.0), 3)),
+                    float(np.round(rng.uniform(-0.8, 0.8), 4)),
+                    float(np.round(rng.uniform(0.0, 40.0), 3)) * 1000.0)
+    plain[2].rlt = (float(np.round(rng.uniform(-20.0, 20.0), 4)),
+                    float(np.round(rng.uniform(-50.0, 50.0), 4)))
     return m
 
 
@@ -497,6 +506,8 @@ def write_chemkin(mech: Mechanism, out_dir: str, stem: str = "mech") -> Tuple[st
             lines.append(f"   PLOG / {pa:g}  {A(Ap, fo):.6E}  {bp:.6f}  {E(Ep):.4f} /")
         if r.lt is not None:
             lines.append(f"   LT / {r.lt[0]:g}  {r.lt[1]:g} /")
+        if r.rlt is not None:
+            lines.append(f"   RLT / {r.rlt[0]:g}  {r.rlt[1]:g} /")
         if r.janev is not None:
             lines.append("   JAN / " + "  ".join(f"{x:.10g}" for x in r.janev) + " /")
         if r.fit1 is not None:

@@ -366,8 +366,7 @@ static double plogDkDT(const hc_mech_desc *m, int r, double kj, double p, double
 }
 
 /* Landau-Teller (LandauTellerRR.cpp:37-99) */
-static double ltK(const hc_mech_desc *m, int r, double T) {
-    const double *a = &m->arr[3 * r], *bc = &m->lt[2 * r];
+static double ltK(const double *a, const double *bc, double T) {
     double lta = a[0];
     if (fabs(a[1]) > VERY_TINY) lta *= pow(T, a[1]);
     double expAgr = 0.0;
@@ -378,8 +377,7 @@ static double ltK(const hc_mech_desc *m, int r, double T) {
     return lta;
 }
 
-static double ltDkDT(const hc_mech_desc *m, int r, double T) {
-    const double *a = &m->arr[3 * r], *bc = &m->lt[2 * r];
+static double ltDkDT(const double *a, const double *bc, double T) {
     double lta = a[0];
     if (fabs(a[1]) > VERY_TINY) lta *= pow(T, a[1]);
     double expArg = 0, deriv = 0;
@@ -462,7 +460,7 @@ static double rateK(const hc_mech_desc *m, int r, double p, double T, const doub
     const double *a = &m->arr[3 * r];
     if (t == HC_RATE_ARRHENIUS) return arrK(a, T);
     if (t == HC_RATE_PLOG) return plogK(m, r, p, T);
-    if (t == HC_RATE_LANDAU_TELLER) return ltK(m, r, T);
+    if (t == HC_RATE_LANDAU_TELLER) return ltK(&m->arr[3 * r], &m->lt[2 * r], T);
     if (t == HC_RATE_JANEV) return janevK(m, r, T);
     if (t == HC_RATE_POWER_SERIES) return pseriesK(m, r, T);
     if (t == HC_RATE_THIRD_BODY) {
@@ -482,7 +480,7 @@ static double rateDkDT(const hc_mech_desc *m, int r, double kj, double p, double
     const double *a = &m->arr[3 * r];
     if (t == HC_RATE_ARRHENIUS || t == HC_RATE_THIRD_BODY) return arrDkDT(a, kj, T);
     if (t == HC_RATE_PLOG) return plogDkDT(m, r, kj, p, T);
-    if (t == HC_RATE_LANDAU_TELLER) return ltDkDT(m, r, T);
+    if (t == HC_RATE_LANDAU_TELLER) return ltDkDT(&m->arr[3 * r], &m->lt[2 * r], T);
     if (t == HC_RATE_JANEV) return janevDkDT(m, r, T);
     if (t == HC_RATE_POWER_SERIES) return pseriesDkDT(m, r, T);
     const double k0 = arrK(&m->arr0[3 * r], T);
@@ -593,9 +591,12 @@ static double DKcDT(const mech_ctx *x, int r, double T) {
 }
 
 /* explicit reverse rate (reversibleReactionWithRevPars::kr): the reverse
-   Arrhenius law, or the third-body one, M times it */
+   Arrhenius law, the third-body one (M times it), or for a Landau-Teller
+   reaction the reverse Landau-Teller law of Chemkin RLT (B, C in xcoef,
+   chemkinFileRead.cpp:441-478, 1507-1512) */
 static double kRevExplicit(const hc_mech_desc *m, int r, double T, const double *c) {
     const double *a = &m->arr_rev[3 * r];
+    if (m->rate_type[r] == HC_RATE_LANDAU_TELLER) return ltK(a, &m->xcoef[9 * r], T);
     if (m->rate_type[r] == HC_RATE_THIRD_BODY) {
         const double M = thirdM(m, r, c);
         return (M * arrK(a, T));
@@ -612,7 +613,11 @@ static double kRev(const mech_ctx *x, int r, double kfwd, double T, const double
 }
 
 static double DkrDT(const mech_ctx *x, int r, double kr, double T, double dkfdT) {
-    if (x->m->reversible[r] == HC_REVERSIBLE_REV) return arrDkDT(&x->m->arr_rev[3 * r], kr, T);
+    if (x->m->reversible[r] == HC_REVERSIBLE_REV) {
+        if (x->m->rate_type[r] == HC_RATE_LANDAU_TELLER)
+            return ltDkDT(&x->m->arr_rev[3 * r], &x->m->xcoef[9 * r], T);
+        return arrDkDT(&x->m->arr_rev[3 * r], kr, T);
+    }
     if (!x->m->reversible[r]) return 0.0;
     const double kc = hmax(Kc(x, r, T), VERY_TINY);
     return (dkfdT - kr * DKcDT(x, r, T)) / kc;

@@ -208,7 +208,7 @@ def test_janev_and_power_series_tables(fitted):
     assert np.array_equal(t.xcoef[f, :4], np.array(rx[f].fit1))
     assert not t.xcoef[f, 4:].any()
     assert t.arr[f, 2] == 0.0 and t.arr[j, 2] > 0.0
-    others = [i for i in range(len(rx)) if i not in (j, f)]
+    others = [i for i in range(len(rx)) if i not in (j, f) and rx[i].rlt is None]
     assert not t.xcoef[others].any()
     import pytest
     with pytest.raises(ValueError, match="JAN"):
@@ -216,3 +216,37 @@ def test_janev_and_power_series_tables(fitted):
                              " JAN / 1 2 3 4 5 6 7 8 9 /"))
     with pytest.raises(ValueError, match="FIT1 takes 4"):
         M.parse_chemkin(_che("H2+O2=2HO 1.0E13 0.0 1000.0\n FIT1 / 1 2 3 /"))
+
+
+def test_reverse_landau_teller_tables(fitted):
+    """LT + REV + RLT: the reverse rate takes REV's A, beta, Ta and RLT's B, C
+    (in xcoef); RLT needs REV before it and LT on the reaction."""
+    t = fitted["tables"]
+    rx = fitted["mech"].reactions
+    k = next(i for i, r in enumerate(rx) if r.rlt is not None)
+    assert t.rate_type[k] == M.RATE_LANDAU_TELLER and t.reversible[k] == M.REVERSIBLE_REV
+    assert np.array_equal(t.lt[k], np.array(rx[k].lt))
+    assert np.array_equal(t.xcoef[k, :2], np.array(rx[k].rlt)) and not t.xcoef[k, 2:].any()
+    assert t.arr_rev[k, 1] == rx[k].rev[1]
+    import pytest
+    with pytest.raises(ValueError, match="must follow the explicit REV"):
+        M.parse_chemkin(_che("H2+O2=2HO 1.0E13 0.0 1000.0\n LT / 1 2 /\n RLT / 1 2 /\n"
+                             " REV / 1.0E12 0.0 0.0 /"))
+    with pytest.raises(ValueError, match="RLT on a reaction without LT"):
+        M.compile_mechanism(*_without(fitted, "   LT / "))
+    with pytest.raises(ValueError, match="needs RLT"):
+        M.compile_mechanism(*_without(fitted, "   RLT / "))
+
+
+def _without(fixture, prefix):
+    """The fixture's files with the mechanism lines that start with `prefix` dropped."""
+    import os
+    import tempfile
+    che, th, tr = fixture["files"]
+    d = tempfile.mkdtemp()
+    text = open(che).read().splitlines()
+    text = [l for l in text if not l.startswith(prefix)]
+    out = os.path.join(d, "chem.inp")
+    with open(out, "w") as f:
+        f.write("\n".join(text) + "\n")
+    return out, th, tr

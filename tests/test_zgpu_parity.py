@@ -473,10 +473,11 @@ def test_temperature_from_energy_vs_reference_golden(name, request):
 
 @pytest.mark.parametrize("kernel", [0, 2])
 def test_fitted_rates_parity_vs_oracle(fitted, kernel):
-    """Janev (JAN) and power-series (FIT1) rates through the cell-group kernel
-    against the oracle (pinned to the reference); over 1e-7 s these cells are
-    well conditioned (one-ulp input changes move T by 6e-10 in the oracle) and
-    take at most 39503 Newton iterations each."""
+    """Janev (JAN), power-series (FIT1) and reverse Landau-Teller (RLT) rates
+    through the cell-group kernel against the oracle (pinned to the
+    reference); over 1e-7 s these cells are well conditioned (one-ulp input
+    changes move T by 1.4e-9 relative in the oracle) and take at most 44060
+    Newton iterations each."""
     t = fitted["tables"]
     T, p, rho, Y = _cells(t, 96, seed=23)
     m = _mech(t)
