@@ -61,6 +61,10 @@ extern "C" {
                                      (LandauTellerRR) */
 #define HC_RATE_JANEV 8     /* A T^b exp(-Ta/T + sum_{n<9} b_n (ln T)^n), Chemkin JAN (JanevRR) */
 #define HC_RATE_POWER_SERIES 9  /* A T^b exp(sum_{n<4} b_n / T^(n+1)), Chemkin FIT1 (powerSeriesRR) */
+#define HC_RATE_COLLISION 10    /* min(1, A T^b exp(-Ta/T)) x0 sqrt(x1 T), Chemkin COLLEFF
+                                   (collisionRR); xcoef = N_A d^2, 8 pi Ru / W_AB, 2 pi Ru / W_AB
+                                   with d the mean Lennard-Jones diameter of the two reactants
+                                   as read (angstrom) and W_AB their reduced molar mass */
 
 /* hc_mech_desc.reversible */
 #define HC_IRREVERSIBLE 0
@@ -119,7 +123,8 @@ typedef struct hc_mech_desc {
        line) and arr = kinf (HIGH); k = k0 F / (1 + Pr). NULL: none */
     const int32_t *activated; /* [nrc] */
     const double *lt;        /* [nrc*2] Landau-Teller B, C (HC_RATE_LANDAU_TELLER); NULL: none */
-    const double *xcoef;     /* [nrc*9] Janev b_0..b_8 or power-series b_0..b_3 (then zeros);
+    const double *xcoef;     /* [nrc*9] Janev b_0..b_8, power-series b_0..b_3 or collision
+                                x0..x2 (then zeros);
                                 for a Landau-Teller reaction with HC_REVERSIBLE_REV, the
                                 reverse rate's B, C (Chemkin RLT): kr is then the
                                 Landau-Teller law on arr_rev and these. NULL: none */

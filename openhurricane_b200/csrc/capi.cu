@@ -290,12 +290,14 @@ static int check_desc(const hc_mech_desc *d) {
     for (int r = 0; r < nrc; ++r) {
         if (d->nf[r] < 0 || d->nf[r] > HC_MAX_SIDE || d->nb[r] < 0 || d->nb[r] > HC_MAX_SIDE)
             return fail(HC_E_INVALID, "reaction side larger than HC_MAX_SIDE");
-        if (d->rate_type[r] < 0 || d->rate_type[r] > HC_RATE_POWER_SERIES)
+        if (d->rate_type[r] < 0 || d->rate_type[r] > HC_RATE_COLLISION)
             return fail(HC_E_INVALID, "unknown rate type");
         if (d->rate_type[r] >= HC_RATE_JANEV) {
-            if (!d->xcoef) return fail(HC_E_INVALID, "Janev / power-series reaction without coefficients");
+            if (!d->xcoef)
+                return fail(HC_E_INVALID, "Janev / power-series / collision reaction without coefficients");
             if (d->reversible[r] == HC_REVERSIBLE_REV)
-                return fail(HC_E_INVALID, "explicit reverse parameters on a Janev / power-series reaction");
+                return fail(HC_E_INVALID,
+                            "explicit reverse parameters on a Janev / power-series / collision reaction");
         }
         if (d->activated && d->activated[r] &&
             (d->rate_type[r] < HC_RATE_LINDEMANN || d->rate_type[r] > HC_RATE_SRI))
@@ -542,7 +544,8 @@ int hc_jit_source(const hc_mech_desc *d, int block, char *buf, int64_t cap, int6
     make_host(d, h);
     if (h.ext)
         return fail(HC_E_UNSUPPORTED,
-                    "no generated kernel for SRI, explicit reverse (REV), PLOG, HIGH, LT, JAN or FIT1 rate laws");
+                    "no generated kernel for SRI, explicit reverse (REV), PLOG, HIGH, LT, JAN, FIT1 or "
+                    "collision rate laws");
     const std::string src = jit_t1_source(h, block);
     *len = (int64_t)src.size();
     if (buf && cap > 0) {
@@ -606,12 +609,12 @@ static int integrate_impl(hc_mech_t m, const hc_opts *opts, int64_t ncells, doub
         return fail(HC_E_UNSUPPORTED,
                     "thread-per-cell kernel needs nsp <= 15, autoUpdateJacobian off, the "
                     "constant-pressure reactor and no SRI or explicit reverse (REV), PLOG, HIGH, "
-                    "LT, JAN or FIT1 rate laws");
+                    "LT, JAN, FIT1 or collision rate laws");
     if (m->kernel == 4 && !(t1_ok && m->t2_ok))
         return fail(HC_E_UNSUPPORTED,
                     "compact thread-per-cell kernel needs nsp <= 15, <= 64 reactions, "
                     "autoUpdateJacobian off, the constant-pressure reactor and no SRI, explicit "
-                    "reverse (REV), PLOG, HIGH, LT, JAN or FIT1 rate laws");
+                    "reverse (REV), PLOG, HIGH, LT, JAN, FIT1 or collision rate laws");
     // automatic choice: the cell group. Per-cell costs in a flow step differ
     // by orders of magnitude, and the step lasts as long as its stiffest
     // cell; the cell group's lanes share each Newton iteration's work and
@@ -636,7 +639,7 @@ static int integrate_impl(hc_mech_t m, const hc_opts *opts, int64_t ncells, doub
         return fail(HC_E_UNSUPPORTED,
                     "generated thread-per-cell kernel needs nsp <= 15, autoUpdateJacobian off, the "
                     "constant-pressure reactor and no SRI, explicit reverse (REV), PLOG, HIGH, LT, "
-                    "JAN or FIT1 rate laws");
+                    "JAN, FIT1 or collision rate laws");
     bool use_jit = t1_ok && m->kernel == 3;
     if (use_jit && !m->jit_tried) {
         // first use: generate, compile and load (host work, no stream operation)
@@ -1516,7 +1519,7 @@ extern "C" int hc_integrate_noalloc(hc_mech_t m, const hc_opts *opts, int64_t nc
         return fail(HC_E_UNSUPPORTED,
                     "hc_integrate_noalloc needs nsp <= 15, <= 64 reactions, autoUpdateJacobian off, "
                     "the constant-pressure reactor and no SRI, explicit reverse (REV), PLOG, HIGH, "
-                    "LT, JAN or FIT1 rate laws");
+                    "LT, JAN, FIT1 or collision rate laws");
     int dev = -1;
     HC_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 256) return fail(HC_E_CUDA, "device ordinal out of range");

@@ -151,12 +151,13 @@ static __device__ __noinline__ double lt_dkdt_global(const double *a, const doub
     return lt_dkdt(k, ldg(&a[1]), ldg(&a[2]), ldg(&bc[0]), ldg(&bc[1]), T);
 }
 
-// Janev and power-series rates: a = A, beta, Ta; x = the reaction's 9 coefficients
+// Janev, power-series and collision rates: a = A, beta, Ta; x = the reaction's 9 coefficients
 static __device__ __noinline__ double xrate_k_global(int type, const double *a, const double *x,
                                                     double T, double logT) {
     double bn[9];
     for (int n = 0; n < 9; ++n) bn[n] = ldg(&x[n]);
     if (type == kJanev) return janev_k(ldg(&a[0]), ldg(&a[1]), ldg(&a[2]), bn, T, logT);
+    if (type == kCollision) return collision_k(ldg(&a[0]), ldg(&a[1]), ldg(&a[2]), bn, T, logT);
     return pseries_k(ldg(&a[0]), ldg(&a[1]), bn, T, logT);
 }
 
@@ -165,6 +166,7 @@ static __device__ __noinline__ double xrate_dkdt_global(int type, const double *
     double bn[9];
     for (int n = 0; n < 9; ++n) bn[n] = ldg(&x[n]);
     if (type == kJanev) return janev_dkdt(k, ldg(&a[1]), ldg(&a[2]), bn, T, logT);
+    if (type == kCollision) return collision_dkdt(k, ldg(&a[1]), ldg(&a[2]), bn, T);
     return pseries_dkdt(k, ldg(&a[1]), bn, T);
 }
 

@@ -27,7 +27,7 @@ constexpr int kMaxSide = 4;
 
 enum RateType : int32_t {
     kArrhenius = 0, kThirdBody = 1, kLindemann = 2, kTroe3 = 3, kTroe4 = 4, kSRI = 5, kPLOG = 6,
-    kLandauTeller = 7, kJanev = 8, kPowerSeries = 9
+    kLandauTeller = 7, kJanev = 8, kPowerSeries = 9, kCollision = 10
 };
 // reversible flags: 1 kr = kf / Kc, 2 kr from explicit reverse Arrhenius parameters
 constexpr int32_t kRevExplicit = 2;
@@ -277,6 +277,22 @@ __device__ __forceinline__ double janev_dkdt(double k, double b, double Ta, cons
         d += n * bn[n] * lp;
     }
     return k * (b + Ta / T + d) / T;
+}
+
+// collision efficiency (collisionRR.hpp:94-107, 146-169, collisionRR.cpp:36-46):
+// k = min(1, A T^b exp(-Ta/T)) Z(T), Z = N_A d^2 sqrt(8 pi (Ru / W_AB) T), and
+// dk/dT = (k > 1 ? k (b + Ta/T) / T : 0) N_A d^2 sqrt(2 pi (Ru / W_AB) / T), both as
+// the reference states them; x = (N_A d^2, 8 pi Ru / W_AB, 2 pi Ru / W_AB)
+__device__ __forceinline__ double collision_k(double A, double b, double Ta, const double *x,
+                                              double T, double logT) {
+    const double g = arrK_log(A, b, Ta, T, logT);   // std::min(1, g)
+    return (g < 1.0 ? g : 1.0) * (x[0] * sqrt(x[1] * T));
+}
+
+__device__ __forceinline__ double collision_dkdt(double k, double b, double Ta, const double *x,
+                                                 double T) {
+    const double invT = 1.0 / hmax(T, kTiny);
+    return (k > 1.0 ? k * invT * (b + Ta * invT) : 0.0) * (x[0] * sqrt(x[2] / T));
 }
 
 // power series (powerSeriesRateRR.cpp:37-74): k = A T^b exp(sum_{n<4} b_n / T^(n+1)),

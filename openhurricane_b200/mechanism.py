@@ -82,6 +82,7 @@ RATE_PLOG = 6
 RATE_LANDAU_TELLER = 7
 RATE_JANEV = 8
 RATE_POWER_SERIES = 9
+RATE_COLLISION = 10
 
 # reversibility codes
 IRREVERSIBLE = 0
@@ -122,6 +123,7 @@ class ParsedReaction:
     high: Optional[Tuple[float, float, float]] = None   # HIGH A, b, E (chemically activated)
     lt: Optional[Tuple[float, float]] = None             # Landau-Teller B, C
     rlt: Optional[Tuple[float, float]] = None            # reverse Landau-Teller B, C (RLT)
+    collision: bool = False                              # COLLEFF: collision efficiency
     named_third: Optional[int] = None                    # species of a (+X) third body
     janev: Optional[List[float]] = None                  # JAN b_0..b_8
     fit1: Optional[List[float]] = None                   # FIT1 b_0..b_3
@@ -305,6 +307,15 @@ def parse_chemkin(che_text: str, species_names: Optional[List[str]] = None):
         for key, val, word in _AUX_RE.findall(line.strip()):
             if word:
                 if word.upper() in ("DUP", "DUPLICATE"):
+                    continue
+                if word.upper() == "COLLEFF":
+                    # chemkinFileRead.cpp:345-371: a bimolecular reaction whose
+                    # main line is the collision efficiency
+                    if cur.kind != "arrhenius":
+                        raise ValueError("COLLEFF cannot be used on a third-body or fall-off reaction")
+                    if len(cur.fwd) != 2:
+                        raise ValueError("The collision reaction should be bimolecular")
+                    cur.collision = True
                     continue
                 raise ValueError(f"unexpected word {word!r} in {line.strip()!r}")
             up = key.upper()
@@ -545,7 +556,32 @@ def compile_mechanism(che_path: str, thermo_path: Optional[str] = None,
             order += o
         third = rx.kind != "arrhenius"
         Afac, Efac = change_unit(order, rx.units_A, rx.units_E, third)
-        if rx.plog is not None:
+        if rx.collision:
+            if rx.rev is not None:
+                raise ValueError("REV cannot be used with a collision rate "
+                                 "(chemkinFileRead.cpp:1557-1561)")
+            if rx.plog is not None or rx.lt is not None or rx.janev is not None \
+                    or rx.fit1 is not None:
+                raise ValueError("COLLEFF with another rate form")
+            # collisionRR: the Arrhenius line is the efficiency; the collision
+            # frequency takes the mean Lennard-Jones diameter of the two
+            # reactants as read (angstrom) and their reduced molar mass
+            # (chemkinFileRead.cpp:360-371, 1552-1556; collisionRR.cpp:36-42,
+            # collisionRR.hpp:94-107)
+            (ia, _), (ib, _) = rx.fwd
+            for i in (ia, ib):
+                if names[i] not in tran:
+                    raise ValueError(f"collision reaction needs the transport data of {names[i]}")
+            d = 0.0
+            d += tran[names[ia]][2]
+            d += tran[names[ib]][2]
+            d /= 2.0
+            WAB = (W[ia] * W[ib]) / (W[ia] + W[ib])
+            RAB = RU / WAB
+            rate_type[r] = RATE_COLLISION
+            arr[r] = (rx.A * Afac, rx.b, rx.E / Efac)
+            xcoef[r, :3] = (NA * (d * d), (8.0 * math.pi) * RAB, (2.0 * math.pi) * RAB)
+        elif rx.plog is not None:
             if rx.rev is not None:
                 raise ValueError("REV cannot be used with a PLOG rate (chemkinFileRead.cpp:1609)")
             # logInterpolationRR::append sorts by pressure after each entry

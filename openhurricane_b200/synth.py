@@ -73,6 +73,7 @@ class Reaction:
     activated: bool = False     # chemically activated: main line = low, HIGH = (A, b, Ea)
     lt: Optional[Tuple[float, float]] = None           # Landau-Teller B, C
     rlt: Optional[Tuple[float, float]] = None          # reverse Landau-Teller B, C (with rev)
+    collision: bool = False                            # COLLEFF: A, b, Ea are the efficiency
     janev: Optional[Tuple[float, ...]] = None          # JAN b_0..b_8
     fit1: Optional[Tuple[float, ...]] = None           # FIT1 b_0..b_3
 
@@ -376,12 +377,18 @@ def extended_mechanism(seed: int = 20241117) -> Mechanism:
     return m
 
 
-def fitted_rates_mechanism(seed: int = 20240901) -> Mechanism:
+def fitted_rates_mechanism(seed: int = 20240901,
+                           collision: Tuple[float, float, float] = (2e-21, 0.0, 0.0)) -> Mechanism:
     """The small mechanism with one reaction on a Janev rate (JAN, nine
     coefficients of powers of ln T) and one on a power-series rate (FIT1,
     four coefficients of powers of 1/T), small enough to keep the rates within
-    a decade or so of the drawn Arrhenius ones, and one Landau-Teller reaction
-    with explicit reverse parameters in the Landau-Teller form (LT, REV, RLT)."""
+    a decade or so of the drawn Arrhenius ones, one Landau-Teller reaction
+    with explicit reverse parameters in the Landau-Teller form (LT, REV, RLT),
+    and one collision-efficiency reaction (COLLEFF) with efficiency A, b, Ea
+    `collision`. With b = Ea = 0 the reference's dk/dT of that reaction is zero;
+    otherwise it is the Arrhenius derivative times dZ/dT, about 1e25 times the
+    rate's own derivative, which stalls the Newton iterations, so integrations
+    use the default and only rate and Jacobian checks use other values."""
     m = small_mechanism(seed)
     rng = np.random.default_rng(seed + 7)
     plain = [r for r in m.reactions if r.kind == "plain"]
@@ -398,6 +405,8 @@ def fitted_rates_mechanism(seed: int = 20240901) -> Mechanism:
                     float(np.round(rng.uniform(0.0, 40.0), 3)) * 1000.0)
     plain[2].rlt = (float(np.round(rng.uniform(-20.0, 20.0), 4)),
                     float(np.round(rng.uniform(-50.0, 50.0), 4)))
+    plain[3].collision = True
+    plain[3].A, plain[3].b, plain[3].Ea = collision
     return m
 
 
@@ -508,6 +517,8 @@ def write_chemkin(mech: Mechanism, out_dir: str, stem: str = "mech") -> Tuple[st
             lines.append(f"   LT / {r.lt[0]:g}  {r.lt[1]:g} /")
         if r.rlt is not None:
             lines.append(f"   RLT / {r.rlt[0]:g}  {r.rlt[1]:g} /")
+        if r.collision:
+            lines.append("   COLLEFF")
         if r.janev is not None:
             lines.append("   JAN / " + "  ".join(f"{x:.10g}" for x in r.janev) + " /")
         if r.fit1 is not None:

@@ -451,6 +451,23 @@ static double pseriesDkDT(const hc_mech_desc *m, int r, double T) {
     return lta * (a[1] + deriv) / T;
 }
 
+/* collision efficiency (Chemkin COLLEFF; collisionRR.hpp:94-107, 146-169,
+   collisionRR.cpp:36-46): k = min(1, Arrhenius) Zb(T), Zb = N_A d^2
+   sqrt(8 pi RAB T); dk/dT = (k > 1 ? Arrhenius DkDT at k : 0) dZb/dT with
+   dZb/dT = N_A d^2 sqrt(2 pi RAB / T), as the reference states them.
+   xcoef = (N_A d^2, 8 pi RAB, 2 pi RAB), RAB = Ru / W_AB, made by the reader */
+static double collisionK(const hc_mech_desc *m, int r, double T) {
+    const double *x = &m->xcoef[9 * r];
+    const double g = arrK(&m->arr[3 * r], T);
+    const double gam = (g < 1.0) ? g : 1.0; /* std::min(1, g) */
+    return gam * (x[0] * sqrt(x[1] * T));
+}
+
+static double collisionDkDT(const hc_mech_desc *m, int r, double kj, double T) {
+    const double *x = &m->xcoef[9 * r];
+    return (kj > 1.0 ? arrDkDT(&m->arr[3 * r], kj, T) : 0.0) * (x[0] * sqrt(x[2] / T));
+}
+
 /* chemically activated bimolecular (Chemkin HIGH,
    chemicallyActicatedBimolecularRR.cpp:36-96): k = k0 F / (1 + Pr) */
 static int activated(const hc_mech_desc *m, int r) { return m->activated && m->activated[r]; }
@@ -463,6 +480,7 @@ static double rateK(const hc_mech_desc *m, int r, double p, double T, const doub
     if (t == HC_RATE_LANDAU_TELLER) return ltK(&m->arr[3 * r], &m->lt[2 * r], T);
     if (t == HC_RATE_JANEV) return janevK(m, r, T);
     if (t == HC_RATE_POWER_SERIES) return pseriesK(m, r, T);
+    if (t == HC_RATE_COLLISION) return collisionK(m, r, T);
     if (t == HC_RATE_THIRD_BODY) {
         const double M = thirdM(m, r, c);
         return (M * arrK(a, T));
@@ -483,6 +501,7 @@ static double rateDkDT(const hc_mech_desc *m, int r, double kj, double p, double
     if (t == HC_RATE_LANDAU_TELLER) return ltDkDT(&m->arr[3 * r], &m->lt[2 * r], T);
     if (t == HC_RATE_JANEV) return janevDkDT(m, r, T);
     if (t == HC_RATE_POWER_SERIES) return pseriesDkDT(m, r, T);
+    if (t == HC_RATE_COLLISION) return collisionDkDT(m, r, kj, T);
     const double k0 = arrK(&m->arr0[3 * r], T);
     const double kinf = arrK(a, T);
     const double Pr = k0 / notZeroD(kinf) * thirdM(m, r, c);

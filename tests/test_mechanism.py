@@ -208,7 +208,8 @@ def test_janev_and_power_series_tables(fitted):
     assert np.array_equal(t.xcoef[f, :4], np.array(rx[f].fit1))
     assert not t.xcoef[f, 4:].any()
     assert t.arr[f, 2] == 0.0 and t.arr[j, 2] > 0.0
-    others = [i for i in range(len(rx)) if i not in (j, f) and rx[i].rlt is None]
+    others = [i for i in range(len(rx)) if i not in (j, f) and rx[i].rlt is None
+              and not rx[i].collision]
     assert not t.xcoef[others].any()
     import pytest
     with pytest.raises(ValueError, match="JAN"):
@@ -250,3 +251,25 @@ def _without(fixture, prefix):
     with open(out, "w") as f:
         f.write("\n".join(text) + "\n")
     return out, th, tr
+
+
+def test_collision_efficiency_tables(fitted):
+    """COLLEFF: the main line is the efficiency; xcoef holds N_A d^2 and
+    8 pi / 2 pi times Ru / W_AB, d the mean collision diameter of the two
+    reactants as read (angstrom), W_AB their reduced molar mass."""
+    t = fitted["tables"]
+    rx = fitted["mech"].reactions
+    k = next(i for i, r in enumerate(rx) if r.collision)
+    assert t.rate_type[k] == M.RATE_COLLISION and t.reversible[k] == M.REVERSIBLE
+    (a, _), (b, _) = ((t.names.index(n), v) for n, v in rx[k].reactants)
+    d = (t.sigma[a] + t.sigma[b]) / 2.0
+    wab = t.W[a] * t.W[b] / (t.W[a] + t.W[b])
+    assert math.isclose(t.xcoef[k, 0], M.NA * d * d, rel_tol=1e-15)
+    assert math.isclose(t.xcoef[k, 1], 8.0 * math.pi * M.RU / wab, rel_tol=1e-15)
+    assert math.isclose(t.xcoef[k, 2], 2.0 * math.pi * M.RU / wab, rel_tol=1e-15)
+    assert not t.xcoef[k, 3:].any()
+    import pytest
+    with pytest.raises(ValueError, match="bimolecular"):
+        M.parse_chemkin(_che("H2+O2+HO=2HO+H 1.0E13 0.0 1000.0\n COLLEFF"))
+    with pytest.raises(ValueError, match="third-body or fall-off"):
+        M.parse_chemkin(_che("H2+O2+M=2HO+M 1.0E13 0.0 1000.0\n COLLEFF"))

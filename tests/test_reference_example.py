@@ -119,16 +119,54 @@ def test_named_third_body_falloff_matches_the_reference(small, tmp_path):
         assert np.array_equal(o[k], ref[k]), k
 
 
+def _fitted_kat(t, case, tmp_path):
+    """Known answers of the reference at six states against the oracle: DyDt,
+    the Jacobian and kf / Kc / kr of every reaction, bit for bit."""
+    from oracle import port, refrun
+    rng = np.random.default_rng(3)
+    T = rng.uniform(800.0, 3000.0, 6)
+    p = rng.uniform(1.0, 5.0, 6) * 101325.0
+    cc = rng.dirichlet(np.full(t.nsp, 0.5), 6).T.copy() * 0.01
+    k = refrun.kat(case, p, T, cc, workdir=str(tmp_path))
+    md = port.MechDesc(t)
+    f, J = port.rhs_jac(md, cc, T, p)
+    assert np.array_equal(f, k["dydt"]) and np.array_equal(J, k["J"])
+    for s in range(6):
+        r = port.rates(md, T[s], cc[:, s], p[s])
+        assert np.array_equal(r[:, 0], k["kf"][s]) and np.array_equal(r[:, 2], k["kr"][s])
+
+
+def test_collision_derivative_branch_matches_the_reference(tmp_path):
+    """A collision-efficiency reaction with b != 0: the reference's dk/dT
+    (Arrhenius derivative at k times dZ/dT) enters the Jacobian; known
+    answers only (integrations with it stall, see synth.fitted_rates_mechanism)."""
+    from oracle import refrun
+    from openhurricane_b200 import mechanism, synth
+    if not refrun.available():
+        pytest.skip("reference binary not built (make -f oracle/Makefile.ref)")
+    files = synth.write_chemkin(synth.fitted_rates_mechanism(collision=(1e-22, 0.5, 0.0)),
+                                str(tmp_path / "m"))
+    t = mechanism.compile_mechanism(*files)
+    r = int(np.where(t.rate_type == mechanism.RATE_COLLISION)[0][0])
+    assert t.arr[r, 1] == 0.5
+    case = str(tmp_path / "case.cont")
+    # a viscous flow model: the reference reads the transport data (the
+    # collision diameters) only then, and dereferences an empty table otherwise
+    refrun.write_case(case, *files, {"atol": 1e-15, "flowModel": "laminarFlow"})
+    _fitted_kat(t, case, tmp_path)
+
+
 def test_fitted_rates_match_the_reference(fitted, tmp_path):
-    """Janev (JAN) and power-series (FIT1) rates: reader and oracle against the
+    """Janev (JAN), power-series (FIT1), reverse Landau-Teller (RLT) and
+    collision-efficiency (COLLEFF) rates: reader and oracle against the
     reference build, by integration and known answers."""
     from oracle import port, refrun
     if not refrun.available():
         pytest.skip("reference binary not built (make -f oracle/Makefile.ref)")
     t = fitted["tables"]
-    assert sorted(set(t.rate_type) & {8, 9}) == [8, 9]
+    assert sorted(set(t.rate_type) & {7, 8, 9, 10}) == [7, 8, 9, 10]
     case = str(tmp_path / "case.cont")
-    refrun.write_case(case, *fitted["files"], {"atol": 1e-15})
+    refrun.write_case(case, *fitted["files"], {"atol": 1e-15, "flowModel": "laminarFlow"})
     from openhurricane_b200 import synth
     c = synth.dirichlet_cells(t.nsp, 12, seed=41)
     rho = synth.mixture_density(t.W, c)
@@ -137,10 +175,4 @@ def test_fitted_rates_match_the_reference(fitted, tmp_path):
     o = port.integrate(md, c.T, c.p, rho, c.Y, 1e-6, opts=port.default_opts(atol=1e-15))
     for k in ("T", "Y", "rho", "c", "subdt"):
         assert np.array_equal(o[k], r[k]), k
-    rng = np.random.default_rng(3)
-    T = rng.uniform(800.0, 3000.0, 6)
-    p = rng.uniform(1.0, 5.0, 6) * 101325.0
-    cc = rng.dirichlet(np.full(t.nsp, 0.5), 6).T.copy() * 0.01
-    k = refrun.kat(case, p, T, cc, workdir=str(tmp_path))
-    f, J = port.rhs_jac(md, cc, T, p)
-    assert np.array_equal(f, k["dydt"]) and np.array_equal(J, k["J"])
+    _fitted_kat(t, case, tmp_path)

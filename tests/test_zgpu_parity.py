@@ -473,11 +473,11 @@ def test_temperature_from_energy_vs_reference_golden(name, request):
 
 @pytest.mark.parametrize("kernel", [0, 2])
 def test_fitted_rates_parity_vs_oracle(fitted, kernel):
-    """Janev (JAN), power-series (FIT1) and reverse Landau-Teller (RLT) rates
-    through the cell-group kernel against the oracle (pinned to the
-    reference); over 1e-7 s these cells are well conditioned (one-ulp input
-    changes move T by 1.4e-9 relative in the oracle) and take at most 44060
-    Newton iterations each."""
+    """Janev (JAN), power-series (FIT1), reverse Landau-Teller (RLT) and
+    collision-efficiency (COLLEFF) rates through the cell-group kernel against
+    the oracle (pinned to the reference); over 1e-7 s these cells are well
+    conditioned (one-ulp input changes move T by 2.5e-9 relative in the
+    oracle) and take at most 39150 Newton iterations each."""
     t = fitted["tables"]
     T, p, rho, Y = _cells(t, 96, seed=23)
     m = _mech(t)
@@ -488,10 +488,18 @@ def test_fitted_rates_parity_vs_oracle(fitted, kernel):
     _assert_close(g, o, f"fitted rates, kernel {kernel}")
 
 
-def test_fitted_rates_rhs_jacobian_vs_oracle(fitted):
+@pytest.mark.parametrize("collision_b", [0.0, 0.5])
+def test_fitted_rates_rhs_jacobian_vs_oracle(fitted, collision_b, tmp_path):
+    """DyDt and the Jacobian of the fitted-rates mechanism; with b = 0.5 on the
+    collision reaction its dk/dT (the reference's Arrhenius derivative at k
+    times dZ/dT) is non-zero."""
     from oracle import port
+    from openhurricane_b200 import mechanism, synth
     dev = _cuda()
     t = fitted["tables"]
+    if collision_b:
+        t = mechanism.compile_mechanism(*synth.write_chemkin(
+            synth.fitted_rates_mechanism(collision=(1e-22, collision_b, 0.0)), str(tmp_path)))
     rng = np.random.default_rng(3)
     n = 16
     T = rng.uniform(800.0, 3000.0, n)
