@@ -27,12 +27,18 @@ and stores inputs and outputs:
                   of its cells answer one-ulp input changes with 1e-6 changes
                   of T); plus KAT states,
                   point-implicit source terms and properties of 16 cells.
+  fitted_ref.npz: the small mechanism with Janev (JAN), power-series (FIT1),
+                  reverse Landau-Teller (LT + REV + RLT) and collision-
+                  efficiency (COLLEFF) reactions (synth.fitted_rates_mechanism),
+                  96 cells, dt = 1e-7 s, run with a viscous flow model (the
+                  reference reads collision diameters only then); plus KAT
+                  states, point-implicit source terms and properties of 16 cells.
 
 The mechanism files are regenerated from their seeds by
 openhurricane_b200.synth at test time; a SHA-256 of the generated text files
 is stored so that a change of the generator is detected.
 
-    python tests/golden/make_golden.py [small] [large] [ext] [cv]   (default: all;
+    python tests/golden/make_golden.py [small] [large] [ext] [cv] [fitted]   (default: all;
     needs oracle/_ref/hurchem_ref)
 """
 import hashlib
@@ -69,11 +75,11 @@ def kat_states(nsp, n, seed):
     return T, p, np.ascontiguousarray(c)
 
 
-def make(name, mech, cells, dt, nkat, prop_cells, out):
+def make(name, mech, cells, dt, nkat, prop_cells, out, flow="EulerFlow"):
     work = tempfile.mkdtemp(prefix="golden_")
     files = synth.write_chemkin(mech, work)
     case = os.path.join(work, "case.cont")
-    refrun.write_case(case, *files, {"atol": 1e-15})
+    refrun.write_case(case, *files, {"atol": 1e-15, "flowModel": flow})
     W = mech.weights()
     rho = synth.mixture_density(W, cells)
     res = refrun.integrate(case, cells.T, cells.p, rho, dt, dt, cells.Y,
@@ -143,7 +149,7 @@ def make_cv(out):
 def main():
     if not refrun.available():
         raise SystemExit("oracle/_ref/hurchem_ref is missing: make -f oracle/Makefile.ref")
-    which = set(sys.argv[1:]) or {"small", "large", "ext", "cv"}
+    which = set(sys.argv[1:]) or {"small", "large", "ext", "cv", "fitted"}
     if "small" in which:
         small = synth.small_mechanism()
         make("small", small, synth.dirichlet_cells(9, 48, seed=101), 1e-6, 8,
@@ -161,6 +167,12 @@ def main():
              synth.dirichlet_cells(9, 16, seed=111), os.path.join(HERE, "ext_ref.npz"))
     if "cv" in which:
         make_cv(os.path.join(HERE, "cv_ref.npz"))
+    if "fitted" in which:
+        # a viscous flow model: the reference reads the collision diameters of
+        # the COLLEFF reaction from the transport table only then
+        make("fitted", synth.fitted_rates_mechanism(), synth.dirichlet_cells(9, 96, seed=23), 1e-7,
+             8, synth.dirichlet_cells(9, 16, seed=115), os.path.join(HERE, "fitted_ref.npz"),
+             flow="laminarFlow")
 
 
 if __name__ == "__main__":

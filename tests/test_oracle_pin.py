@@ -30,13 +30,13 @@ def _load(name):
     return np.load(os.path.join(HERE, "golden", f"{name}_ref.npz"))
 
 
-@pytest.mark.parametrize("name", ["small", "large", "ext"])
+@pytest.mark.parametrize("name", ["small", "large", "ext", "fitted"])
 def test_generator_reproduces_golden_mechanism(name, request):
     mk = request.getfixturevalue(name)
     assert _sha(mk["files"]) == str(_load(name)["sha"])
 
 
-@pytest.mark.parametrize("name", ["small", "large", "ext"])
+@pytest.mark.parametrize("name", ["small", "large", "ext", "fitted"])
 def test_oracle_integration_bit_exact_vs_reference_golden(name, request):
     from oracle import port
     mk = request.getfixturevalue(name)
@@ -48,7 +48,7 @@ def test_oracle_integration_bit_exact_vs_reference_golden(name, request):
         assert np.array_equal(o[k], g["out_" + k]), k
 
 
-@pytest.mark.parametrize("name", ["small", "large", "ext"])
+@pytest.mark.parametrize("name", ["small", "large", "ext", "fitted"])
 def test_oracle_kernels_bit_exact_vs_reference_golden(name, request):
     from oracle import port
     mk = request.getfixturevalue(name)
@@ -63,7 +63,7 @@ def test_oracle_kernels_bit_exact_vs_reference_golden(name, request):
                               g["kat_rates"][s])
 
 
-@pytest.mark.parametrize("name", ["small", "large", "ext"])
+@pytest.mark.parametrize("name", ["small", "large", "ext", "fitted"])
 def test_property_oracle_vs_reference_golden(name, request):
     from oracle import props_oracle
     mk = request.getfixturevalue(name)
@@ -94,7 +94,7 @@ def test_oracle_bit_exact_vs_reference_binary(small):
     assert o["status"][0] == 1 and r["status"][0] == 1
 
 
-@pytest.mark.parametrize("name", ["small", "large", "ext"])
+@pytest.mark.parametrize("name", ["small", "large", "ext", "fitted"])
 def test_point_implicit_oracle_vs_reference_golden(name, request):
     """Ri and the diagonal source Jacobian of calculateSourceTermsImp."""
     from oracle import srcimp_oracle
@@ -107,7 +107,7 @@ def test_point_implicit_oracle_vs_reference_golden(name, request):
     assert (np.abs(o["diag"] - ref) / scale).max() < 1e-14
 
 
-@pytest.mark.parametrize("name", ["small", "large", "ext"])
+@pytest.mark.parametrize("name", ["small", "large", "ext", "fitted"])
 def test_temperature_from_enthalpy_oracle_vs_reference_golden(name, request):
     """thermoList::THa_p: Newton on the mixture enthalpy with the reference's
     tolerance, iteration cap and [TLow, THigh] clamp."""

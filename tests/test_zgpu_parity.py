@@ -243,16 +243,17 @@ def test_large_mechanism_parity_vs_oracle(large, kernel, block):
     _assert_close(g, o, "large")
 
 
-@pytest.mark.parametrize("name", ["small", "large", "ext"])
+@pytest.mark.parametrize("name", ["small", "large", "ext", "fitted"])
 def test_against_reference_golden_outputs(name, request):
     """The reference's own outputs (default rtol 1e-4, atol 1e-15): most cells
     agree to the parity tolerance and every cell agrees to the solver's rtol."""
     mk = request.getfixturevalue(name)
     g0 = _golden(name)
     m = _mech(mk["tables"])
-    # the extended mechanism's reference cells take up to 40734 Newton
-    # iterations each; a cap bounds a cell that would take another path
-    cap = dict(max_newton_total=1000000) if name == "ext" else {}
+    # the extended and fitted-rates mechanisms' reference cells take up to
+    # some 40000 Newton iterations each; a cap bounds a cell that would take
+    # another path
+    cap = dict(max_newton_total=1000000) if name in ("ext", "fitted") else {}
     g = _gpu_integrate(m, g0["in_T"], g0["in_p"], g0["in_rho"], g0["in_Y"], float(g0["dt"]),
                        atol=1e-15, **cap)
     dT = np.abs(g["T"] - g0["out_T"]) / g0["out_T"]
@@ -262,7 +263,7 @@ def test_against_reference_golden_outputs(name, request):
     assert ok.mean() >= 0.9, f"{ok.mean():.3f} of cells within parity tolerance"
 
 
-@pytest.mark.parametrize("name", ["small", "large", "ext"])
+@pytest.mark.parametrize("name", ["small", "large", "ext", "fitted"])
 def test_rhs_jacobian_vs_reference_golden(name, request):
     mk = request.getfixturevalue(name)
     g0 = _golden(name)
@@ -420,7 +421,7 @@ def test_graph_captured_step_matches_eager(which, small, large):
     del g
 
 
-@pytest.mark.parametrize("name", ["small", "large", "ext"])
+@pytest.mark.parametrize("name", ["small", "large", "ext", "fitted"])
 def test_point_implicit_source_terms_vs_reference_golden(name, request):
     """hc_source_terms_imp against the reference's calculateSourceTermsImp
     outputs and the oracle on fresh cells."""
