@@ -331,10 +331,13 @@ static int check_desc(const hc_mech_desc *d) {
         }
         if (d->reversible[r] == HC_REVERSIBLE_REV) {
             if (!d->arr_rev) return fail(HC_E_INVALID, "REV reaction without reverse parameters");
-            // reversibleReactionWithRevPars takes Arrhenius and third-body rates only
-            // (chemkinFileRead.cpp:1387-1444)
-            if (d->rate_type[r] != HC_RATE_ARRHENIUS && d->rate_type[r] != HC_RATE_THIRD_BODY)
-                return fail(HC_E_INVALID, "explicit reverse parameters on a fall-off reaction");
+            // reversibleReactionWithRevPars takes Arrhenius, third-body and, with
+            // the reverse B, C of RLT, Landau-Teller rates (chemkinFileRead.cpp:1387-1444,
+            // 1502-1516)
+            if (d->rate_type[r] != HC_RATE_ARRHENIUS && d->rate_type[r] != HC_RATE_THIRD_BODY &&
+                d->rate_type[r] != HC_RATE_LANDAU_TELLER)
+                return fail(HC_E_INVALID,
+                            "explicit reverse parameters on a fall-off or PLOG reaction");
         }
         for (int k = 0; k < d->nf[r]; ++k)
             if (d->fidx[HC_MAX_SIDE * r + k] < 0 || d->fidx[HC_MAX_SIDE * r + k] >= nsp)

@@ -85,6 +85,36 @@ def test_mechanism_checks_of_the_extended_rate_forms_without_gpu(ext):
     bad(bad_code, b"reversibility")
 
 
+def test_mechanism_checks_of_the_fitted_rate_forms_without_gpu(fitted):
+    """Janev, power-series, reverse Landau-Teller and collision reactions: the
+    generated thread-per-cell kernel refuses them; their coefficient table,
+    explicit reverse parameters where they cannot be, and unknown rate codes
+    are rejected on the host."""
+    import copy
+    from openhurricane_b200 import _capi
+    lib = _capi.load()
+    n = C.c_int64()
+    a = _capi.DescArrays(fitted["tables"])
+    assert lib.hc_jit_source(C.byref(a.desc), 64, None, 0, C.byref(n)) == -3
+    assert b"collision" in lib.hc_last_error()
+
+    def bad(mutate, msg):
+        b = _capi.DescArrays(copy.deepcopy(fitted["tables"]))
+        mutate(b)
+        assert lib.hc_jit_source(C.byref(b.desc), 64, None, 0, C.byref(n)) == -1
+        assert msg in lib.hc_last_error()
+
+    bad(lambda b: setattr(b.desc, "xcoef", None), b"without coefficients")
+
+    def rev_on_collision(b):
+        b.arrays["reversible"][b.arrays["rate_type"] == 10] = 2
+    bad(rev_on_collision, b"explicit reverse parameters on a Janev / power-series / collision")
+
+    def unknown_code(b):
+        b.arrays["rate_type"][b.arrays["rate_type"] == 10] = 11
+    bad(unknown_code, b"unknown rate type")
+
+
 def test_state_api_rejects_null_handles_without_gpu():
     from openhurricane_b200 import _capi
     lib = _capi.load()
