@@ -6,6 +6,7 @@
 //   "L A b Ta B C T"  -> lt_k, lt_dkdt
 //   "J A b Ta b_0 .. b_8 T"  -> janev_k, janev_dkdt
 //   "F A b b_0 .. b_3 T"  -> pseries_k, pseries_dkdt
+//   "K A b Ta x_0 x_1 x_2 T"  -> collision_k, collision_dkdt
 #include <cmath>
 #include <cstdio>
 
@@ -39,6 +40,12 @@ int main() {
             if (std::scanf("%lf %lf %lf %lf %lf %lf", &A, &b, &Ta, &B, &C, &T) != 6) return 1;
             const double k = hc::lt_k(A, b, Ta, B, C, T, std::log(T));
             std::printf("%.17g %.17g\n", k, hc::lt_dkdt(k, b, Ta, B, C, T));
+        } else if (kind[0] == 'K') {
+            double A, b, Ta, x[3], T;
+            if (std::scanf("%lf %lf %lf %lf %lf %lf %lf", &A, &b, &Ta, &x[0], &x[1], &x[2], &T) != 7)
+                return 1;
+            const double k = hc::collision_k(A, b, Ta, x, T, std::log(T));
+            std::printf("%.17g %.17g\n", k, hc::collision_dkdt(k, b, Ta, x, T));
         } else if (kind[0] == 'J' || kind[0] == 'F') {
             const int nb = kind[0] == 'J' ? 9 : 4;
             double A, b, Ta = 0.0, bn[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, T;

@@ -254,3 +254,32 @@ def test_janev_and_power_series_helpers_match_the_reference(exe):
         dk = k * (b - sum((n + 1) * fn[n] / math.pow(T, n + 1) for n in range(4))) / T
         assert abs(g[0] - k) <= 1e-13 * abs(k)
         assert abs(g[1] - dk) <= 1e-12 * abs(dk) + 1e-14 * abs(k) / T
+
+
+def test_collision_helpers_match_the_reference(exe):
+    """collisionRR (collisionRR.hpp:94-107, 146-169): k = min(1, Arrhenius) Zb,
+    dk/dT = (k > 1 ? k (b + Ta/T) / T : 0) dZb/dT, on both sides of k = 1 and
+    of the efficiency's cap at 1."""
+    rng = np.random.default_rng(12)
+    cases = []
+    for i in range(120):
+        A = float(10.0 ** rng.uniform(-34, 2))
+        b = float(rng.choice([0.0, rng.uniform(-1, 1)]))
+        Ta = float(rng.choice([0.0, rng.uniform(0, 2e4)]))
+        x = (float(6.02214076e23 * rng.uniform(2, 6) ** 2), float(rng.uniform(2e3, 5e5)),
+             0.0)
+        x = (x[0], x[1], x[1] / 4.0)
+        cases.append((A, b, Ta, x, float(rng.uniform(300, 3000))))
+    txt = "".join(f"K {A!r} {b!r} {Ta!r} {x[0]!r} {x[1]!r} {x[2]!r} {T!r}\n"
+                  for A, b, Ta, x, T in cases)
+    out = subprocess.run([exe], input=txt, capture_output=True, text=True, check=True).stdout
+    got = np.array([[float(v) for v in l.split()] for l in out.strip().splitlines()])
+    seen = set()
+    for (A, b, Ta, x, T), g in zip(cases, got):
+        gam = min(1.0, A * math.pow(T, b) * math.exp(-Ta / T))
+        k = gam * (x[0] * math.sqrt(x[1] * T))
+        dk = (k * (b + Ta / T) / T if k > 1.0 else 0.0) * (x[0] * math.sqrt(x[2] / T))
+        seen.add((gam == 1.0, k > 1.0))
+        assert abs(g[0] - k) <= 1e-13 * abs(k)
+        assert abs(g[1] - dk) <= 1e-12 * abs(dk) + 1e-300
+    assert {(False, True), (False, False), (True, True)} <= seen
