@@ -183,37 +183,3 @@ def test_async_source_terms_return_before_the_results_and_overlap_host_work(smal
     assert torch.equal(RRi, ref)
     # the call enqueues about 2 x 190 MB of copies: it must not have waited for them
     assert t_call < 0.5 * t_dev, (t_call, t_dev)
-
-
-def test_property_records_match_species_major_fields(large):
-    """calchaicp / calcTransportProperties records ([Y..., T, p] in;
-    [h..., cp] and [D..., mu, kappa] out) against hc_properties on the same
-    cells, device and host forms, bit for bit."""
-    from openhurricane_b200 import _capi
-    from openhurricane_b200.chemistry import Mechanism
-    dev = _dev()
-    t = large["tables"]
-    m = Mechanism(t)
-    n = 1037
-    T, p, rho, Y = _cells(t, n, seed=816)
-    d = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
-    ref = m.properties(d(T), d(p), d(Y))
-    rec = np.ascontiguousarray(np.concatenate([Y.T, T[:, None], p[:, None]], axis=1))
-    hc = torch.empty((n, t.nsp + 1), dtype=torch.float64, device=dev)
-    dmk = torch.empty((n, t.nsp + 2), dtype=torch.float64, device=dev)
-    vp = lambda x: C.c_void_p(x.data_ptr())
-    lib = _capi.load()
-    rec_d = d(rec)
-    assert lib.hc_properties_aos(m.handle, n, vp(rec_d), vp(hc), vp(dmk),
-                                 C.c_void_p(torch.cuda.current_stream().cuda_stream)) == 0
-    torch.cuda.synchronize()
-    hc, dmk = hc.cpu().numpy(), dmk.cpu().numpy()
-    assert np.array_equal(hc[:, :-1], ref["ha"].cpu().numpy().T)
-    assert np.array_equal(hc[:, -1], ref["cp"].cpu().numpy())
-    assert np.array_equal(dmk[:, :-2], ref["D"].cpu().numpy().T)
-    assert np.array_equal(dmk[:, -2], ref["mu"].cpu().numpy())
-    assert np.array_equal(dmk[:, -1], ref["kappa"].cpu().numpy())
-    hc_h = np.zeros((n, t.nsp + 1))
-    assert lib.hc_properties_aos_host(m.handle, n, rec.ctypes.data_as(C.c_void_p),
-                                      hc_h.ctypes.data_as(C.c_void_p), None, None) == 0
-    assert np.array_equal(hc_h, hc)
