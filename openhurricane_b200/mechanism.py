@@ -38,11 +38,12 @@ Arrhenius and third-body reactions; non-stoichiometric orders (FORD, RORD).
 pressure-dependent Arrhenius tables (PLOG, logInterpolationRR) on reactions
 without a third body; chemically activated bimolecular reactions (HIGH,
 chemicallyActicatedBimolecularRR) with any fall-off function; Landau-Teller
-rates (LT, LandauTellerRR); Janev (JAN, JanevRR) and power-series (FIT1,
-powerSeriesRR) rates. The reference's other forms (RLT, TDEP, ...) are
-rejected with NotImplementedError, and so is CHEB, whose
-reference implementation does not evaluate the Chebyshev fit (see
-parse_chemkin).
+rates (LT, LandauTellerRR), with REV also in the reverse direction (RLT);
+Janev (JAN, JanevRR), power-series (FIT1, powerSeriesRR) and collision-
+efficiency (COLLEFF, collisionRR) rates. TDEP, XSMI, MOME and EXCI, which the
+reference's reader refuses too, are rejected with NotImplementedError, and
+so is CHEB, whose reference implementation does not evaluate the Chebyshev
+fit (see parse_chemkin).
 """
 from __future__ import annotations
 
@@ -96,9 +97,9 @@ UNITS_E = {"CAL": "CAL", "CAL/MOLE": "CAL", "EVOL": "EVOL", "EVOLTS": "EVOL", "J
            "JOULES/MOLE": "JOUL", "KCAL": "KCAL", "KCAL/MOLE": "KCAL", "KELV": "KELV",
            "KELVINS": "KELV", "KJOU": "KJOU", "KJOULES/MOLE": "KJOU"}
 ELECTRON_VOLT = 1.6021766208e-19    # J (physicalConstant.hpp:59,114)
-# auxiliary keywords of the reference's reader that this reader does not take
-_UNSUPPORTED_AUX = {"CHEB", "PCHEB", "TCHEB", "TDEP",
-                    "XSMI", "MOME", "EXCI", "COLLEFF"}
+# auxiliary keywords that the reference's own reader refuses as not yet supported
+# (chemkinFileRead.cpp:530-558)
+_UNSUPPORTED_AUX = {"TDEP", "XSMI", "MOME", "EXCI"}
 
 
 @dataclasses.dataclass
@@ -334,7 +335,8 @@ def parse_chemkin(che_text: str, species_names: Optional[List[str]] = None):
                     "evaluate the Chebyshev fit (0.001*log10 of the sum, default ranges, "
                     "a 1e-15 divisor in dk/dT); reactions using it are not taken")
             if up in _UNSUPPORTED_AUX:
-                raise NotImplementedError(f"rate form {up} is not supported by this reader")
+                raise NotImplementedError(f"rate form {up} is not supported (nor by the "
+                                          "reference's reader)")
             if up == "LOW":
                 cur.low = (_read_real(v[0]), _read_real(v[1]), _read_real(v[2]))
             elif up == "TROE":

@@ -273,3 +273,10 @@ def test_collision_efficiency_tables(fitted):
         M.parse_chemkin(_che("H2+O2+HO=2HO+H 1.0E13 0.0 1000.0\n COLLEFF"))
     with pytest.raises(ValueError, match="third-body or fall-off"):
         M.parse_chemkin(_che("H2+O2+M=2HO+M 1.0E13 0.0 1000.0\n COLLEFF"))
+
+
+def test_forms_the_reference_refuses_are_refused():
+    import pytest
+    for key in ("TDEP / H2 /", "XSMI / 1.0 /", "MOME / 1.0 /", "EXCI / 1.0 /"):
+        with pytest.raises(NotImplementedError, match="not supported"):
+            M.parse_chemkin(_che("H2+O2=2HO 1.0E13 0.0 1000.0\n " + key))
