@@ -186,9 +186,13 @@ void hc_default_opts(hc_opts *opts);
  * 3 = thread per cell generated for this mechanism (every index and
  * coefficient a literal; compiled with NVRTC for sm_100a on first use, which
  * must precede any stream capture), 4 = compact thread per cell (mechanism
- * in the kernel's constant parameter bank: nsp <= 15, <= 64 reactions);
+ * in the kernel's constant parameter bank: nsp <= 15, <= 64 reactions),
+ * 5 = thread per cell generated for this mechanism with the Newton matrix
+ * I - dt J assembled column by column from register-held rates and written
+ * once per entry, no divisions on the common path and a small instruction
+ * footprint (NVRTC on first use, like 3);
  * block = threads per block of the thread-per-cell kernels (32, 64 or 128). Set by the autotuner (openhurricane_b200/autotune.py).
- * The thread-per-cell kernels (1, 3, 4) take nsp <= 15, the constant-pressure
+ * The thread-per-cell kernels (1, 3, 4, 5) take nsp <= 15, the constant-pressure
  * reactor and the common rate forms (Arrhenius, third body, Lindemann / Troe
  * fall-off); a call that asks for one of them outside that range fails with
  * HC_E_UNSUPPORTED. The cell group takes everything hc_mech_create accepts.
@@ -203,6 +207,12 @@ int hc_jit_source(const hc_mech_desc *desc, int block, char *buf, int64_t cap, i
 /* Compile that source with NVRTC for sm_100a without loading it (host only);
  * cubin_bytes receives the size of the compiled image. */
 int hc_jit_compile(const hc_mech_desc *desc, int block, int64_t *cubin_bytes);
+/* The same for a chosen generated kernel: 3 (thread per cell, Jacobian
+ * scattered into shared memory) or 5 (thread per cell, Newton matrix
+ * assembled column by column from register-held rates). */
+int hc_jit_source_kernel(const hc_mech_desc *desc, int kernel, int block, char *buf, int64_t cap,
+                         int64_t *len);
+int hc_jit_compile_kernel(const hc_mech_desc *desc, int kernel, int block, int64_t *cubin_bytes);
 
 /* Upload a mechanism; selects the compiled kernel variant for nsp. */
 int hc_mech_create(const hc_mech_desc *desc, hc_mech_t *out);

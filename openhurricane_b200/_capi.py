@@ -100,6 +100,10 @@ SIGNATURES = {
     "hc_default_opts": (None, [C.POINTER(HcOpts)]),
     "hc_set_tuning": (C.c_int, [_VP, C.c_int, C.c_int]),
     "hc_jit_compile": (C.c_int, [C.POINTER(HcMechDesc), C.c_int, C.POINTER(C.c_int64)]),
+    "hc_jit_compile_kernel": (C.c_int, [C.POINTER(HcMechDesc), C.c_int, C.c_int,
+                                        C.POINTER(C.c_int64)]),
+    "hc_jit_source_kernel": (C.c_int, [C.POINTER(HcMechDesc), C.c_int, C.c_int, C.c_char_p,
+                                       C.c_int64, C.POINTER(C.c_int64)]),
     "hc_jit_source": (C.c_int, [C.POINTER(HcMechDesc), C.c_int, C.c_char_p, C.c_int64,
                                 C.POINTER(C.c_int64)]),
     "hc_mech_create": (C.c_int, [C.POINTER(HcMechDesc), C.POINTER(_VP)]),

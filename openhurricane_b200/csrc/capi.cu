@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -21,6 +22,7 @@
 #include "jit.h"
 #include "surrogate.cuh"
 #include "variants.h"
+#include "wcell.cuh"
 
 using namespace hc;
 
@@ -94,6 +96,13 @@ struct hc_mech_s {
     JitKernel jit;
     bool jit_tried = false;
     std::string jit_err;
+    // the compact thread-per-cell kernel (kernel 5, generated)
+    JitKernel jit5;
+    bool jit5_tried = false;
+    std::string jit5_err;
+    // the warp-per-cell kernel's tables (kernel 6)
+    WMech w{};
+    bool w_ok = false;
 };
 
 namespace {
@@ -175,6 +184,7 @@ static void make_host(const hc_mech_desc *d, HostMech &h) {
     };
     h.nsp = nsp;
     h.nrc = nrc;
+    h.perm.assign(perm.begin(), perm.end());
     h.W.assign(d->W, d->W + nsp);
     h.Trange.assign(d->Trange, d->Trange + 3 * (size_t)nsp);
     h.nasa.assign(d->nasa, d->nasa + 14 * (size_t)nsp);
@@ -277,6 +287,156 @@ static bool pack_t2(const HostMech &h, const hc_mech_desc *d, T2Mech &t) {
         R.eff_end = (int16_t)ne;
     }
     (void)d;
+    return true;
+}
+
+// The mechanism in the warp-per-cell kernel's tables (wcell.cuh): species
+// NASA-7 pre-multiplied by W and the polynomial factors, reactions in the
+// mechanism's own order (the order the reference sums f and J in), each
+// species' participation list, the third-body / fall-off reactions.
+struct WHost {
+    std::vector<double> th, rd, eff, raw, lnu, xj;
+    std::vector<int32_t> ri, lptr, lent, tbl;
+    int nsp = 0, nrc = 0, nrc32 = 0, njob = 0, njob32 = 0;
+    double glim = 0.0;
+};
+
+static bool pack_w(const HostMech &h, WHost &w) {
+    if (h.nsp + 1 > 16 || h.ext) return false;
+    const int nsp = h.nsp, nrc = h.nrc, S = HC_MAX_SIDE;
+    w.nsp = nsp;
+    w.nrc = nrc;
+    w.nrc32 = std::max(32, ((nrc + 31) / 32) * 32);
+    const int n32 = w.nrc32;
+    w.th.assign((size_t)kWTHn * 32, 0.0);
+    auto T = [&](int f, int i) -> double & { return w.th[(size_t)f * 32 + i]; };
+    for (int i = 0; i < nsp; ++i) {
+        const double W = h.W[i];
+        T(kWtl, i) = h.Trange[3 * i];
+        T(kWtc, i) = h.Trange[3 * i + 1];
+        T(kWth, i) = h.Trange[3 * i + 2];
+        T(kWW, i) = W;
+        for (int rg = 0; rg < 2; ++rg) {
+            const double *a = &h.nasa[14 * i + 7 * rg];
+            const int b = kWrange + rg * kWRangeN;
+            for (int k = 0; k < 5; ++k) T(b + k, i) = W * a[k] / (k + 1);
+            T(b + 5, i) = W * a[5];
+            T(b + 6, i) = W * a[0];
+            for (int k = 1; k < 5; ++k) T(b + 6 + k, i) = W * a[k] / k;
+            T(b + 11, i) = W * a[6];
+            for (int k = 0; k < 5; ++k) T(b + 12 + k, i) = W * a[k];
+            for (int k = 1; k < 5; ++k) T(b + 16 + k, i) = k * W * a[k];
+        }
+    }
+    std::vector<int> dev(nrc);   // mechanism order -> device order
+    for (int r = 0; r < nrc; ++r) dev[((int)h.perm.size() == nrc) ? h.perm[r] : r] = r;
+    w.rd.assign((size_t)kWRDn * n32, 0.0);
+    w.ri.assign((size_t)kWRIn * n32, 0);
+    w.eff.assign((size_t)std::max(nrc, 1) * nsp, 0.0);
+    double worst = 1.0;
+    for (int o = 0; o < nrc; ++o) {
+        const int r = dev[o];
+        const int type = h.rate_type[r], nf = h.nf[r], nb = h.nb[r];
+        if (nf + nb > 8) return false;
+        // round-major: [round][field][32]
+        auto RI = [&](int f) -> int32_t & { return w.ri[((size_t)(o >> 5) * kWRIn + f) * 32 + (o & 31)]; };
+        auto RD = [&](int f) -> double & { return w.rd[((size_t)(o >> 5) * kWRDn + f) * 32 + (o & 31)]; };
+        RI(kWtype) = type;
+        RI(kWrev) = h.reversible[r] ? 1 : 0;
+        RI(kWnf) = nf;
+        RI(kWnb) = nb;
+        RD(kWA) = h.arr[3 * r];
+        RD(kWb) = h.arr[3 * r + 1];
+        RD(kWTa) = h.arr[3 * r + 2];
+        RD(kWA0) = h.arr0[3 * r];
+        RD(kWb0) = h.arr0[3 * r + 1];
+        RD(kWTa0) = h.arr0[3 * r + 2];
+        if (type == HC_RATE_TROE3 || type == HC_RATE_TROE4) {
+            RD(kWalpha) = h.troe[4 * r];
+            RD(kWTsss) = h.troe[4 * r + 1];
+            RD(kWTs) = h.troe[4 * r + 2];
+            RD(kWiTsss) = 1.0 / h.troe[4 * r + 1];
+            RD(kWiTs) = 1.0 / h.troe[4 * r + 2];
+            RD(kWTss) = h.troe[4 * r + 3];
+        }
+        RD(kWs) = h.sum_stoi[r];
+        double sn = 0.0;
+        for (int k = 0; k < nf; ++k) {
+            RI(kWidx + k) = h.fidx[S * r + k];
+            RD(kWnu + k) = -h.fnu[S * r + k];
+            RD(kWord + k) = h.ford[S * r + k];
+            sn += std::fabs(h.fnu[S * r + k]);
+        }
+        for (int k = 0; k < nb; ++k) {
+            RI(kWidx + nf + k) = h.bidx[S * r + k];
+            RD(kWnu + nf + k) = h.bnu[S * r + k];
+            RD(kWord + nf + k) = h.bord[S * r + k];
+            sn += std::fabs(h.bnu[S * r + k]);
+        }
+        for (int k = nf + nb; k < 8; ++k) RD(kWord + k) = 1.0;
+        if (h.reversible[r]) worst = std::max(worst, sn);
+        if (type != HC_RATE_ARRHENIUS) {
+            for (int i = 0; i < nsp; ++i) w.eff[(size_t)o * nsp + i] = h.eff[(size_t)r * nsp + i];
+            w.tbl.push_back(o);
+        }
+    }
+    // participation lists: per entry the reaction, the species' position
+    // among its participants, their number, a third-body flag, the
+    // participants' columns (8 bits each) and the species' signed coefficient
+    // exponential jobs: each reaction's Arrhenius factor, then the fall-off
+    // reactions' low-pressure factor and Troe centering terms
+    {
+        std::vector<std::array<double, 3>> jobs(nrc);
+        for (int o = 0; o < nrc; ++o) {
+            const int r = dev[o];
+            jobs[o] = {h.arr[3 * r + 1], -h.arr[3 * r + 2], 0.0};
+        }
+        for (int o = 0; o < nrc; ++o) {
+            const int r = dev[o], type = h.rate_type[r];
+            if (type < HC_RATE_LINDEMANN) continue;
+            w.ri[((size_t)(o >> 5) * kWRIn + kWxj) * 32 + (o & 31)] = (int32_t)jobs.size();
+            jobs.push_back({h.arr0[3 * r + 1], -h.arr0[3 * r + 2], 0.0});
+            if (type == HC_RATE_TROE3 || type == HC_RATE_TROE4) {
+                jobs.push_back({0.0, 0.0, -1.0 / h.troe[4 * r + 1]});
+                jobs.push_back({0.0, 0.0, -1.0 / h.troe[4 * r + 2]});
+                if (type == HC_RATE_TROE4) jobs.push_back({0.0, -h.troe[4 * r + 3], 0.0});
+            }
+        }
+        w.njob = (int)jobs.size();
+        w.njob32 = std::max(32, ((w.njob + 31) / 32) * 32);
+        w.xj.assign((size_t)3 * w.njob32, 0.0);
+        for (int j = 0; j < w.njob; ++j)
+            for (int f = 0; f < 3; ++f) w.xj[((size_t)(j >> 5) * 3 + f) * 32 + (j & 31)] = jobs[j][f];
+    }
+    w.lptr.assign(nsp + 1, 0);
+    w.lent.clear();
+    w.lnu.clear();
+    for (int i = 0; i < nsp; ++i) {
+        w.lptr[i] = (int32_t)w.lnu.size();
+        for (int o = 0; o < nrc; ++o) {
+            auto RI = [&](int f) { return w.ri[((size_t)(o >> 5) * kWRIn + f) * 32 + (o & 31)]; };
+            auto RD = [&](int f) { return w.rd[((size_t)(o >> 5) * kWRDn + f) * 32 + (o & 31)]; };
+            const int np = RI(kWnf) + RI(kWnb);
+            uint32_t c[2] = {0u, 0u};
+            for (int k = 0; k < np; ++k) c[k >> 2] |= (uint32_t)RI(kWidx + k) << (8 * (k & 3));
+            for (int k = 0; k < np; ++k) {
+                if (RI(kWidx + k) != i) continue;
+                w.lent.push_back(o | (k << 16) | (np << 20) | ((RI(kWtype) != HC_RATE_ARRHENIUS) ? (1 << 24) : 0));
+                w.lent.push_back((int32_t)c[0]);
+                w.lent.push_back((int32_t)c[1]);
+                w.lnu.push_back(RD(kWnu + k));
+            }
+        }
+    }
+    w.lptr[nsp] = (int32_t)w.lnu.size();
+    if (w.lnu.empty()) {
+        w.lent.assign(3, 0);
+        w.lnu.push_back(0.0);
+    }
+    if (nrc >= (1 << 16)) return false;
+    if (w.tbl.empty()) w.tbl.push_back(0);
+    w.raw.assign(h.nasa.begin(), h.nasa.end());
+    w.glim = std::min(300.0, 580.0 / worst);
     return true;
 }
 
@@ -441,6 +601,37 @@ int hc_mech_create(const hc_mech_desc *d, hc_mech_t *out) {
     up(hm.lt.data(), 2 * (size_t)nrc, &dm.lt);
     up(hm.xcoef.data(), 9 * (size_t)nrc, &dm.xcoef);
     up(hm.plog_ptr.data(), (size_t)nrc + 1, &dm.plog_ptr);
+    {
+        // the warp-per-cell kernel's tables (nsp + 1 <= 32, the common rate forms)
+        WHost wh;
+        if (pack_w(hm, wh)) {
+            WMech &w = m->w;
+            w.nsp = wh.nsp;
+            w.nrc = wh.nrc;
+            w.nrc32 = wh.nrc32;
+            w.ntb = (int)wh.tbl.size();
+            if (wh.tbl.size() == 1) {
+                const int o = wh.tbl[0];
+                if (wh.nrc == 0 || wh.ri[((size_t)(o >> 5) * kWRIn + kWtype) * 32 + (o & 31)] == HC_RATE_ARRHENIUS)
+                    w.ntb = 0;   // placeholder entry only
+            }
+            w.nent = (int)wh.lnu.size();
+            w.njob = wh.njob;
+            w.njob32 = wh.njob32;
+            w.glim = wh.glim;
+            up(wh.th.data(), wh.th.size(), &w.th);
+            up(wh.rd.data(), wh.rd.size(), &w.rd);
+            up(wh.ri.data(), wh.ri.size(), &w.ri);
+            up(wh.eff.data(), wh.eff.size(), &w.eff);
+            up(wh.lptr.data(), wh.lptr.size(), &w.lptr);
+            up(wh.lent.data(), wh.lent.size(), &w.lent);
+            up(wh.lnu.data(), wh.lnu.size(), &w.lnu);
+            up(wh.xj.data(), wh.xj.size(), &w.xj);
+            up(wh.tbl.data(), wh.tbl.size(), &w.tbl);
+            up(wh.raw.data(), wh.raw.size(), &w.raw);
+            m->w_ok = (rc == HC_OK);
+        }
+    }
     up(hm.plog_p.data(), hm.plog_p.size(), &dm.plog_p);
     up(hm.plog_arr.data(), hm.plog_arr.size(), &dm.plog_arr);
     up(p_eff.data(), (size_t)nrc * nsp, &dm.eff);
@@ -509,35 +700,39 @@ int hc_mech_create(const hc_mech_desc *d, hc_mech_t *out) {
 
 int hc_set_tuning(hc_mech_t m, int kernel, int block) {
     if (!m) return fail(HC_E_INVALID, "null mechanism");
-    if (kernel < 0 || kernel > 4) return fail(HC_E_INVALID, "kernel must be 0 .. 4");
+    if (kernel < 0 || kernel > 6) return fail(HC_E_INVALID, "kernel must be 0 .. 6");
     if (block != 32 && block != 64 && block != 128)
         return fail(HC_E_INVALID, "block must be 32, 64 or 128");
     if (block != m->block) {
-        m->jit_tried = false;   // the generated kernel is built per block size
+        m->jit_tried = false;   // the generated kernels are built per block size
         m->jit = JitKernel();
+        m->jit5_tried = false;
+        m->jit5 = JitKernel();
     }
     m->kernel = kernel;
     m->block = block;
     return HC_OK;
 }
 
-int hc_jit_compile(const hc_mech_desc *d, int block, int64_t *cubin_bytes) {
+int hc_jit_compile_kernel(const hc_mech_desc *d, int kernel, int block, int64_t *cubin_bytes) {
     if (!d || !cubin_bytes) return fail(HC_E_INVALID, "null argument");
     int64_t len = 0;
-    int rc = hc_jit_source(d, block, nullptr, 0, &len);
+    int rc = hc_jit_source_kernel(d, kernel, block, nullptr, 0, &len);
     if (rc != HC_OK) return rc;
     HostMech h;
     make_host(d, h);
     std::vector<char> cubin;
     std::string err;
-    rc = jit_compile(jit_t1_source(h, block), cubin, err);
+    rc = jit_compile(kernel == 5 ? jit_t3_source(h, block) : jit_t1_source(h, block), cubin, err);
     if (rc != HC_OK) return fail(rc, err);
     *cubin_bytes = (int64_t)cubin.size();
     return HC_OK;
 }
 
-int hc_jit_source(const hc_mech_desc *d, int block, char *buf, int64_t cap, int64_t *len) {
+int hc_jit_source_kernel(const hc_mech_desc *d, int kernel, int block, char *buf, int64_t cap,
+                         int64_t *len) {
     if (!d || !len) return fail(HC_E_INVALID, "null argument");
+    if (kernel != 3 && kernel != 5) return fail(HC_E_INVALID, "generated kernels are 3 and 5");
     const int vrc = check_desc(d);
     if (vrc != HC_OK) return vrc;
     if (d->nsp + 1 > 16) return fail(HC_E_UNSUPPORTED, "no generated kernel for nsp + 1 > 16");
@@ -549,7 +744,7 @@ int hc_jit_source(const hc_mech_desc *d, int block, char *buf, int64_t cap, int6
         return fail(HC_E_UNSUPPORTED,
                     "no generated kernel for SRI, explicit reverse (REV), PLOG, HIGH, LT, JAN, FIT1 or "
                     "collision rate laws");
-    const std::string src = jit_t1_source(h, block);
+    const std::string src = (kernel == 5) ? jit_t3_source(h, block) : jit_t1_source(h, block);
     *len = (int64_t)src.size();
     if (buf && cap > 0) {
         const size_t n = std::min<size_t>((size_t)cap - 1, src.size());
@@ -557,6 +752,14 @@ int hc_jit_source(const hc_mech_desc *d, int block, char *buf, int64_t cap, int6
         buf[n] = 0;
     }
     return HC_OK;
+}
+
+int hc_jit_compile(const hc_mech_desc *d, int block, int64_t *cubin_bytes) {
+    return hc_jit_compile_kernel(d, 3, block, cubin_bytes);
+}
+
+int hc_jit_source(const hc_mech_desc *d, int block, char *buf, int64_t cap, int64_t *len) {
+    return hc_jit_source_kernel(d, 3, block, buf, cap, len);
 }
 
 int hc_mech_destroy(hc_mech_t m) {
@@ -637,6 +840,41 @@ static int integrate_impl(hc_mech_t m, const hc_opts *opts, int64_t ncells, doub
             m->ylast_cells = (size_t)ncells;
         }
         return variant_integrate_t2(N, m->t2, m->num_sms, P, io, m->ylast, m->block, st, g_err);
+    }
+    if (m->kernel == 6) {
+        if (!m->w_ok || opts->reactor != 0)
+            return fail(HC_E_UNSUPPORTED,
+                        "warp-per-cell kernel needs nsp + 1 <= 16, the constant-pressure reactor and no "
+                        "SRI, explicit reverse (REV), PLOG, HIGH, LT, JAN, FIT1 or collision rate laws");
+        return launch_integrate_w(m->w, m->num_sms, P, io, st, g_err);
+    }
+    if (m->kernel == 5 && !t1_ok)
+        return fail(HC_E_UNSUPPORTED,
+                    "direct-assembly thread-per-cell kernel needs nsp <= 15, autoUpdateJacobian off, "
+                    "the constant-pressure reactor and no SRI, explicit reverse (REV), PLOG, HIGH, "
+                    "LT, JAN, FIT1 or collision rate laws");
+    if (t1_ok && m->kernel == 5) {
+        if (!m->jit5_tried) {
+            // first use: generate, compile and load (host work, no stream operation)
+            m->jit5_tried = true;
+            std::string err;
+            if (jit_build_t3(m->host, m->block, &m->jit5, err) != HC_OK) {
+                m->jit5 = JitKernel();
+                m->jit5_err = err;
+            }
+        }
+        if (!m->jit5.func) return fail(HC_E_UNSUPPORTED, "generated kernel unavailable: " + m->jit5_err);
+        if (m->ylast_cells < (size_t)ncells) {
+            // grows only: a first call with a new, larger size synchronises the
+            // stream and must therefore come before any stream capture
+            HC_CUDA(cudaStreamSynchronize(st));
+            if (m->ylast) HC_CUDA(cudaFree(m->ylast));
+            m->ylast = nullptr;
+            m->ylast_cells = 0;
+            HC_CUDA(cudaMalloc(&m->ylast, sizeof(double) * 2 * 16 * (size_t)ncells));
+            m->ylast_cells = (size_t)ncells;
+        }
+        return jit_launch_t1(m->jit5, m->num_sms, P, io, m->ylast, st, g_err);
     }
     if (m->kernel == 3 && !t1_ok)
         return fail(HC_E_UNSUPPORTED,

@@ -48,6 +48,7 @@ struct T1Cell {
     // temperature sits in the last slot of the state vector; species 0..nsp-1
     // come first and any padding species between them and T stay zero
     static constexpr int TI = N - 1;
+    static constexpr bool kAssemblesA = false;
     const DevMech &m;
     double *s;      // block shared memory base
     int *piv;       // block pivot base

@@ -54,6 +54,7 @@ struct T2Mech {
 template <int N, int B>
 struct T2Cell {
     static constexpr int TI = N - 1;
+    static constexpr bool kAssemblesA = false;
     static constexpr int kJ = 0, kF = N * N, kC = kF + N, kG = kC + N, kD = kG + N;
     static constexpr int kSlots = kD + N;   // doubles per thread
     const T2Mech &m;

@@ -66,6 +66,7 @@ std::string jit_t1_source(const HostMech &h, int block) {
       << "namespace hc {\n"
       << "struct JitCell {\n"
       << "  static constexpr int N = " << N << ", B = " << block << ";\n"
+      << "  static constexpr bool kAssemblesA = false;\n"
       << "  int nsp = " << nsp << ";\n"
       << "  double *J;\n"
       << "  double f_[N];\n"
@@ -447,7 +448,7 @@ int jit_compile(const std::string &src, std::vector<char> &cubin, std::string &e
         return HC_E_UNSUPPORTED;
     }
     nvrtcProgram_t prog = nullptr;
-    if (nv.create(&prog, src.c_str(), "hc_jit_t1.cu", kJitHeaderCount, kJitHeaders,
+    if (nv.create(&prog, src.c_str(), "hc_jit.cu", kJitHeaderCount, kJitHeaders,
                   kJitHeaderNames) != 0) {
         err = "nvrtcCreateProgram failed";
         return HC_E_CUDA;
@@ -472,12 +473,11 @@ int jit_compile(const std::string &src, std::vector<char> &cubin, std::string &e
     return HC_OK;
 }
 
-int jit_build_t1(const HostMech &h, int block, JitKernel *out, std::string &err) {
-    const int N = h.nsp + 1;
-    if (N > 16) {
-        err = "specialised thread-per-cell kernel is built for nsp + 1 <= 16";
-        return HC_E_UNSUPPORTED;
-    }
+namespace {
+
+// compile (cached per device and source text) and load one generated kernel
+int jit_build(const std::string &src, const char *fname, int N, int slots, int block, JitKernel *out,
+              std::string &err) {
     const Driver &dr = driver();
     if (!dr.ok) {
         err = "CUDA driver entry points unavailable";
@@ -485,7 +485,6 @@ int jit_build_t1(const HostMech &h, int block, JitKernel *out, std::string &err)
     }
     int dev = 0;
     cudaGetDevice(&dev);
-    const std::string src = jit_t1_source(h, block);
     const std::string key = std::to_string(dev) + "\n" + src;
     void *module = nullptr, *func = nullptr;
     {
@@ -506,7 +505,7 @@ int jit_build_t1(const HostMech &h, int block, JitKernel *out, std::string &err)
             return HC_E_CUDA;
         }
         CUfunction f = nullptr;
-        if (dr.get(&f, mod, "hc_jit_t1") != CUDA_SUCCESS) {
+        if (dr.get(&f, mod, fname) != CUDA_SUCCESS) {
             err = "cuModuleGetFunction failed for the generated kernel";
             return HC_E_CUDA;
         }
@@ -515,7 +514,7 @@ int jit_build_t1(const HostMech &h, int block, JitKernel *out, std::string &err)
         std::lock_guard<std::mutex> lk(g_cache_mu);
         g_cache[key] = CacheEntry{module, func};
     }
-    const size_t smem = sizeof(double) * (size_t)N * N * block;
+    const size_t smem = sizeof(double) * (size_t)slots * block;
     if (dr.set_attr(static_cast<CUfunction>(func), CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES,
                     (int)smem) != CUDA_SUCCESS) {
         err = "cuFuncSetAttribute failed for the generated kernel";
@@ -533,6 +532,26 @@ int jit_build_t1(const HostMech &h, int block, JitKernel *out, std::string &err)
     out->smem = smem;
     out->per_sm = per_sm;
     return HC_OK;
+}
+
+}  // namespace
+
+int jit_build_t1(const HostMech &h, int block, JitKernel *out, std::string &err) {
+    const int N = h.nsp + 1;
+    if (N > 16) {
+        err = "specialised thread-per-cell kernel is built for nsp + 1 <= 16";
+        return HC_E_UNSUPPORTED;
+    }
+    return jit_build(jit_t1_source(h, block), "hc_jit_t1", N, N * N, block, out, err);
+}
+
+int jit_build_t3(const HostMech &h, int block, JitKernel *out, std::string &err) {
+    const int N = h.nsp + 1;
+    if (N > 16) {
+        err = "direct-assembly thread-per-cell kernel is built for nsp + 1 <= 16";
+        return HC_E_UNSUPPORTED;
+    }
+    return jit_build(jit_t3_source(h, block), "hc_jit_t3", N, t3_slots(h.nsp), block, out, err);
 }
 
 int jit_launch_t1(const JitKernel &k, int num_sms, const IntegratorParams &P, const CellIO &io,

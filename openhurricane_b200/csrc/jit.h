@@ -24,6 +24,8 @@ struct HostMech {
     std::vector<double> xcoef;             // [nrc*9] Janev / power-series coefficients
     std::vector<int32_t> plog_ptr;         // [nrc+1], in device reaction order
     std::vector<double> plog_p, plog_arr;
+    // device reaction r is reaction perm[r] of the mechanism as given
+    std::vector<int32_t> perm;
     // the mechanism uses rate forms only the cell-group kernels evaluate
     // (SRI fall-off, explicit reverse parameters, PLOG tables, chemically
     // activated and Landau-Teller rates)
@@ -39,11 +41,17 @@ struct JitKernel {
 };
 
 std::string jit_t1_source(const HostMech &h, int block);
+// the compact thread-per-cell kernel (kernel 5, jit_t3.cu, t4_cell.cuh) and
+// its shared memory per thread in doubles
+std::string jit_t3_source(const HostMech &h, int block);
+int t3_slots(int nsp);
 // NVRTC compile of generated source to an sm_100a cubin (host only)
 int jit_compile(const std::string &src, std::vector<char> &cubin, std::string &err);
 // compile (NVRTC, sm_100a) and load the thread-per-cell kernel for h;
 // modules are cached per source text for the life of the process
 int jit_build_t1(const HostMech &h, int block, JitKernel *out, std::string &err);
+// the same for the compact kernel (kernel 5)
+int jit_build_t3(const HostMech &h, int block, JitKernel *out, std::string &err);
 int jit_launch_t1(const JitKernel &k, int num_sms, const IntegratorParams &P, const CellIO &io,
                   double *ylast, cudaStream_t st, std::string &err);
 

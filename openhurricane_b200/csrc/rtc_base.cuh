@@ -40,13 +40,48 @@ __device__ __forceinline__ bool finite(double x) { return !isnan(x) && !isinf(x)
 // x^y, with the exponents mechanisms use in practice done exactly as a
 // correctly rounded pow returns them (y = 1: x; y = 2: one rounded multiply;
 // y = 0: 1; y = -1: one rounded division); any other exponent calls pow().
+// pow() out of line: one copy per kernel however many call sites use it
+// (the inline expansion is a few KB of instructions per site)
+#if defined(__CUDACC__) || defined(__CUDACC_RTC__)
+#define HC_NOINLINE __noinline__
+#else
+#define HC_NOINLINE __attribute__((noinline))   // host builds of the device code
+#endif
+static __device__ HC_NOINLINE double pow_out(double x, double y) { return pow(x, y); }
+
 __device__ __forceinline__ double pow_n(double x, double y) {
     if (y == 1.0) return x;
     if (y == 2.0) return x * x;
     if (y == 0.0) return 1.0;
     if (y == -1.0) return 1.0 / x;
-    return pow(x, y);
+    return pow_out(x, y);
 }
+
+// 1/b without a branch to a slow path: the hardware approximation (PTX
+// rcp.approx.ftz.f64) refined by three Newton-Raphson steps r <- r + r (1 - b r),
+// each of which doubles the number of correct bits (Markstein, IBM J. Res.
+// Dev. 34 (1990) 111-119); the result is within a few ulp of the correctly
+// rounded reciprocal. Zero, infinity and NaN keep the approximation's own
+// result (+-inf, +-0, NaN), as do subnormal b (flushed: +-inf).
+__device__ __forceinline__ double frcp(double b) {
+#ifdef __CUDA_ARCH__
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(b));
+    double x = r;
+    x = fma(x, fma(-b, x, 1.0), x);
+    x = fma(x, fma(-b, x, 1.0), x);
+    x = fma(x, fma(-b, x, 1.0), x);
+    return (r != 0.0 && !isinf(r)) ? x : r;
+#else
+    return 1.0 / b;   // host builds of the device code (arithmetic checks on the CPU)
+#endif
+}
+
+// a / b as a * frcp(b) (at most a few ulp from the correctly rounded quotient)
+__device__ __forceinline__ double fdiv(double a, double b) { return a * frcp(b); }
+
+// x^y for x > 0 as exp(y ln x), without pow's out-of-line accurate path
+__device__ __forceinline__ double fpow_pos(double x, double y) { return exp(y * log(x)); }
 
 __device__ __forceinline__ double conc_pow(double c, double ord) {
     return pow_n(hmax(c, 0.0), ord);

@@ -7,6 +7,9 @@
 //   void evaluate(const double (&y)[N], bool jac)   f (and J) at y
 //   double F(int i);                            f_i of the last evaluation
 //   void factor(double dt);                     LU of I - dt J, pivoted
+//   static constexpr bool kAssemblesA;          true: evaluate(y, jac, dt) writes
+//                                               I - dt J itself and factor()
+//                                               only factors it
 //   void solve(double (&b)[N]);                 b <- (I - dt J)^-1 b
 //
 // The reference's nested loops (cell -> ODE interval -> step -> step
@@ -34,7 +37,11 @@ enum T1State : int {
     kT1Done
 };
 
-template <int N, class Cell>
+// Lockstep: every thread of the block passes one block barrier per trip of
+// the main loop (threads without a cell keep looping until the whole block is
+// done), so that the block's warps run the heavy block together and share
+// its instruction fetches.
+template <int N, bool Lockstep = false, class Cell>
 __device__ __forceinline__ void t1_run(Cell &cell, const IntegratorParams &P, const CellIO &io,
                                        double *__restrict__ ylast) {
     constexpr int TI = N - 1;
@@ -69,39 +76,42 @@ __device__ __forceinline__ void t1_run(Cell &cell, const IntegratorParams &P, co
                             rr += yi[i] * cell.W(i);
                         }
                     }
+                    const double irr = frcp(hmax(rr, kTiny));
                     double ys = 0.0;
 #pragma unroll
                     for (int i = 0; i < N; ++i)
                         if (i < nsp) {
-                            yi[i] = yi[i] * cell.W(i) / hmax(rr, kTiny);
+                            yi[i] = yi[i] * cell.W(i) * irr;
                             ys += yi[i];
                         }
+                    const double iys = frcp(ys);
                     if (ys != 1.0) {
 #pragma unroll
                         for (int i = 0; i < N; ++i)
-                            if (i < nsp) yi[i] /= ys;
+                            if (i < nsp) yi[i] *= iys;
                     }
                     double wsum = 0.0;
 #pragma unroll
                     for (int i = 0; i < N; ++i)
-                        if (i < nsp) wsum += yi[i] / cell.W(i);
-                    const double Rm = kRu / (1.0 / hmax(wsum, kVeryTiny));
+                        if (i < nsp) wsum += yi[i] * (1.0 / cell.W(i));
+                    const double Rm = kRu * hmax(wsum, kVeryTiny);
                     const double Tn = y[TI];
                     const double rho0 = io.rho[cellid];
+                    const double itstep = frcp(tstep);
 #pragma unroll
                     for (int i = 0; i < N; ++i) {
                         if (i < nsp) {
                             const double Wi = cell.W(i);
                             const int64_t at = (int64_t)i * io.ncells + cellid;
                             if (io.Ri) {
-                                const double c0 = rho0 * io.Y[at] / Wi;
-                                io.Ri[at] = (y[i] - c0) / tstep * Wi;
+                                const double c0 = rho0 * io.Y[at] * (1.0 / Wi);
+                                io.Ri[at] = (y[i] - c0) * itstep * Wi;
                             }
                             io.Y[at] = yi[i];
                         }
                     }
                     io.T[cellid] = Tn;
-                    io.rho[cellid] = p / (Rm * Tn);
+                    io.rho[cellid] = fdiv(p, Rm * Tn);
                     io.subdt[cellid] = sub;
                     if (io.status) io.status[cellid] = cstatus;
                     if (io.cost) io.cost[cellid] = n_newton;
@@ -140,7 +150,7 @@ __device__ __forceinline__ void t1_run(Cell &cell, const IntegratorParams &P, co
 #pragma unroll
                 for (int i = 0; i < N; ++i) {
                     y[i] = 0.0;
-                    if (i < nsp) y[i] = rho0 * io.Y[(int64_t)i * io.ncells + cellid] / cell.W(i);
+                    if (i < nsp) y[i] = rho0 * io.Y[(int64_t)i * io.ncells + cellid] * (1.0 / cell.W(i));
                 }
                 y[TI] = Ti;
                 p = io.p[cellid];
@@ -215,7 +225,7 @@ __device__ __forceinline__ void t1_run(Cell &cell, const IntegratorParams &P, co
                     continue;
                 }
                 if (error > 1.0) {
-                    const double scale = hmax(P.safescale * pow(error, -P.alphainc), P.minscale);
+                    const double scale = hmax(P.safescale * fpow_pos(error, -P.alphainc), P.minscale);
                     adt *= scale;
                     if (adt <= kVeryTiny) {
                         cstatus |= 4;
@@ -231,7 +241,7 @@ __device__ __forceinline__ void t1_run(Cell &cell, const IntegratorParams &P, co
                 for (int i = 0; i < N; ++i) y[i] = yk[i];
                 ++n_steps;
                 if (error > P.err_accept_limit)
-                    dt = hmin(hmax(P.safescale * pow(error, -P.alphainc), P.minscale), P.maxscale) * adt;
+                    dt = hmin(hmax(P.safescale * fpow_pos(error, -P.alphainc), P.minscale), P.maxscale) * adt;
                 else
                     dt = hmax(P.safescale * P.maxscale * adt, adt);
                 dtReached = t;
@@ -245,11 +255,21 @@ __device__ __forceinline__ void t1_run(Cell &cell, const IntegratorParams &P, co
                 }
             }
         }
-        if (state == kT1Done) break;      // no cell left for this thread
-        if (guard >= 64 && state != kT1Newton && state != kT1Err0) continue;
+        if constexpr (Lockstep) {
+            if (!__syncthreads_or(state != kT1Done)) break;   // the whole block is done
+            if (state != kT1Newton && state != kT1Err0) continue;
+        } else {
+            if (state == kT1Done) break;      // no cell left for this thread
+            if (guard >= 64 && state != kT1Newton && state != kT1Err0) continue;
+        }
         // ---------------- heavy block: J at yk, LU, solve
         const bool newton = (state == kT1Newton);
-        cell.evaluate(yk, newton);
+        if constexpr (Cell::kAssemblesA) {
+            // the cell writes the Newton matrix I - dt J while it evaluates J
+            cell.evaluate(yk, newton, lts0);
+        } else {
+            cell.evaluate(yk, newton);
+        }
         if (newton) {
             ++n_jac;
             cell.factor(lts0);
@@ -276,11 +296,11 @@ __device__ __forceinline__ void t1_run(Cell &cell, const IntegratorParams &P, co
                 for (int i = 0; i < N; ++i) {
                     yk[i] += b[i];
                     const double tol = P.atol + P.rtol * hmax(fabs(yk[i]), fabs(yk[i]));
-                    maxErr = hmax(maxErr, fabs(b[i]) / tol);
+                    maxErr = hmax(maxErr, fabs(b[i]) * frcp(tol));
                 }
                 bool fail = false;
                 if (ncount > 0) {
-                    const double diver = maxErr / hmax(lastErr, kTiny);
+                    const double diver = maxErr * frcp(hmax(lastErr, kTiny));
                     if (diver > 2 && ncount > 5) fail = true;
                 }
                 if (fail) {
@@ -305,8 +325,8 @@ __device__ __forceinline__ void t1_run(Cell &cell, const IntegratorParams &P, co
                     } else {
                         // 3-point error estimate (ImplicitEuler.cpp:121-140)
                         const double dtn = lts0, dtn1 = lts1;
-                        const double f1 = 2.0 / (dtn * (dtn + dtn1));
-                        const double f2 = 2.0 / (dtn1 * (dtn + dtn1));
+                        const double f1 = 2.0 * frcp(dtn * (dtn + dtn1));
+                        const double f2 = 2.0 * frcp(dtn1 * (dtn + dtn1));
                         const double LTEF = (dtn * dtn) * 0.5;
                         double me = 0.0;
                         bool nan_y = false;
@@ -317,7 +337,7 @@ __device__ __forceinline__ void t1_run(Cell &cell, const IntegratorParams &P, co
                             if (isnan(yk[i])) nan_y = true;
                             const double tol =
                                 P.atol_inc + P.rtol_inc * hmax(fabs(y[i]), fabs(yk[i]));
-                            me = hmax(me, fabs(e) / tol);
+                            me = hmax(me, fabs(e) * frcp(tol));
                         }
                         error = nan_y ? 1.5 : me;
                         state = kT1AttemptEnd;
@@ -334,7 +354,7 @@ __device__ __forceinline__ void t1_run(Cell &cell, const IntegratorParams &P, co
                 const double e = yk[i] - y[i] - lts0 * cell.F(i);
                 if (isnan(yk[i])) nan_y = true;
                 const double tol = P.atol_inc + P.rtol_inc * hmax(fabs(y[i]), fabs(yk[i]));
-                me = hmax(me, fabs(e) / tol);
+                me = hmax(me, fabs(e) * frcp(tol));
             }
             error = nan_y ? 1.5 : me;
             state = kT1AttemptEnd;
