@@ -53,6 +53,7 @@ METRIC = "chem cells/s per flow step, plain FP64 vs gated surrogate @ max|ΔT|<5
 UNIT = "cells/s"
 WORKLOAD_CELLS = {"batched": 1048576, "small": 4096, "large": 262144}
 L2_FLUSH_BYTES = 256 << 20
+SUR_STEPS = 3            # timed gated-surrogate steps (fixed, whatever --steps)
 # DRAM bytes (read + write) per cell of one integrator launch on the 9-species
 # mechanism: ncu dram__bytes_read.sum + dram__bytes_write.sum of
 # integrate_kernel<10,32> over 5328 cells (profiles/integrator_group_kernel_small.md),
@@ -179,6 +180,25 @@ def reference_cpu(wl, target_seconds: float, cores: int, sample_offset: int = 0)
 
 
 # ----------------------------------------------------------------------------- GPU arm
+def tune_launch(mech, wl, dev):
+    """The autotuner (openhurricane_b200/autotune.py) over the integrator
+    kernels that take this mechanism, on a strided sample of the workload's
+    cells with each cell's Newton iterations capped (equal work per cell, a
+    fraction of a second per trial)."""
+    import torch
+    from openhurricane_b200 import _capi, autotune, workloads
+    d = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+    m = min(wl.n, 16384)
+    idx = np.linspace(0, wl.n - 1, m).astype(np.int64)
+    o = _capi.default_opts(max_newton_total=400, **workloads.SOLVER_OPTS)
+    dt = torch.full((m,), wl.dt, dtype=torch.float64, device=dev)
+    r = autotune.autotune(mech, d(wl.T[idx]), d(wl.p[idx]), d(wl.rho[idx]), d(wl.Y[:, idx]), dt,
+                          opts=o, sample=m, repeats=2)
+    return {"kernel": r["kernel"], "block": r["block"], "source": "autotuner",
+            "sample_cells": r["sample_cells"], "newton_cap_per_cell": 400,
+            "trials": r["trials"]}
+
+
 def run_ours(args, ws, rank, local):
     import torch
     import ctypes as C
@@ -187,6 +207,8 @@ def run_ours(args, ws, rank, local):
 
     if not torch.cuda.is_available():
         raise RuntimeError("bench.py needs a CUDA device")
+    t_start = time.perf_counter()
+    elapsed = lambda: time.perf_counter() - t_start
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     dist = None
@@ -200,9 +222,13 @@ def run_ours(args, ws, rank, local):
     ncells = args.cells or WORKLOAD_CELLS[name]
     wl = build_workload(name, ncells, seed_offset=rank)
     mech = Mechanism(wl.tables)
+    n, nsp = wl.n, wl.tables.nsp
+    tuning = None
     if args.kernel is not None:
         mech.set_tuning(args.kernel, args.block)
-    n, nsp = wl.n, wl.tables.nsp
+        tuning = {"kernel": args.kernel, "block": args.block, "source": "--kernel"}
+    else:
+        tuning = tune_launch(mech, wl, dev)
     d = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
     T0, p0, rho0, Y0 = d(wl.T), d(wl.p), d(wl.rho), d(wl.Y)
     flow = Flow(T0.clone(), p0, rho0.clone(), Y0.clone())
@@ -215,15 +241,21 @@ def run_ours(args, ws, rank, local):
         flow.T.copy_(T0)
         flow.rho.copy_(rho0)
         flow.Y.copy_(Y0)
-        cs.dtInit = None
+        if cs.dtInit is not None:
+            cs.dtInit.copy_(dt)     # in place: a captured step reads this buffer
 
     # warm-up: the first call also fixes the stiffness order for later steps
     counters = None
+    t_w = time.perf_counter()
     for w in range(args.warmup):
         restore()
         cs.solveUpdate(dt, 1.0, counters=(w == args.warmup - 1))
     torch.cuda.synchronize()
+    warm_s = (time.perf_counter() - t_w) / args.warmup
     counters = dict(cs.last_counters)
+    # the timed step is one replay of the captured flow step (queue reset,
+    # integrator launch, stiffness re-ordering)
+    graph = cs.capture_update(dt, 1.0) if args.graph else None
 
     fm = workloads.flop_model(wl.tables)
     flops_per_launch = workloads.work_flops(counters, fm)
@@ -239,7 +271,10 @@ def run_ours(args, ws, rank, local):
         restore()
         flush.fill_(float(k))
         ev[k][0].record(stream)
-        cs.solveUpdate(dt, 1.0)
+        if graph is not None:
+            graph.replay()
+        else:
+            cs.solveUpdate(dt, 1.0)
         ev[k][1].record(stream)
     torch.cuda.synchronize()
     if dist:
@@ -297,10 +332,21 @@ def run_ours(args, ws, rank, local):
     h2d = n * (5 + nsp) * 8
     d2h = n * (3 + nsp) * 8 + n * 4
 
+    step_s = ms_local / args.steps * 1e-3
     sur = None
     if args.surrogate and name == "batched":
+        # fixed work, whatever --steps: sample generation (FP64 integrations
+        # of sur_samples cells), training, and SUR_STEPS timed gated steps
+        # (at worst every cell rejected: a plain step each)
+        est = step_s * (args.sur_samples / n + SUR_STEPS + 1) + 2e-6 * args.sur_epochs * args.sur_samples
+        if elapsed() + est > args.budget_s - 60:
+            sur = {"skipped": f"wall-clock budget: needs about {est:.0f} s, "
+                              f"{args.budget_s - elapsed():.0f} s left of --budget-s {args.budget_s:g}"}
+    if args.surrogate and name == "batched" and sur is None:
         sur = surrogate_leg(args, wl, mech, (T0, p0, rho0, Y0), dt, fp64_ref,
                             ms_local / args.steps, flush, rank)
+    if graph is not None:
+        del graph
 
     props = None
     if name == "large":
@@ -323,7 +369,8 @@ def run_ours(args, ws, rank, local):
         cores = _host_cores()
         cpu = None
         if not args.no_cpu_baseline:
-            cb = reference_cpu(wl, args.cpu_seconds, cores)
+            cpu_s = max(2.0, min(args.cpu_seconds, args.budget_s - elapsed() - 30.0))
+            cb = reference_cpu(wl, cpu_s, cores)
             if cb is not None:
                 v, m, secs = cb
                 cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
@@ -348,6 +395,8 @@ def run_ours(args, ws, rank, local):
                                         "(no FP64 figure in the measured peaks file)",
                          "kernel_ms": kernel_ms, "flops_per_launch": flops_per_launch},
             "counters": counters,
+            "tuning": tuning,
+            "wall_s": {"warmup_step": warm_s, "run_so_far": elapsed()},
             "clocks": clk,
             "cpu_baseline": cpu,
             "surrogate": sur,
@@ -445,7 +494,7 @@ def surrogate_leg(args, wl, mech, fields0, dt, fp64_ref, plain_ms, flush, rank):
     restore()
     sur.step(flow, dt, opts=opts)     # warm-up
     ms, rej = [], []
-    for k in range(args.steps):
+    for k in range(SUR_STEPS):
         restore()
         flush.fill_(float(k))
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -521,6 +570,92 @@ def run_reference(args, ws, rank):
     }
 
 
+# ----------------------------------------------------------------------------- profiling cases
+def run_profile(args):
+    """One small, fixed piece of work for an ncu capture or a quick timing
+    (no JSON bench line): `integrate` one hc_integrate launch of --cells
+    seeded cells of --workload (strided from its cell set) with a per-cell
+    Newton cap --cap (0: none) and --kernel / --block; `gemm` the surrogate's
+    BF16 tcgen05 GEMM on --gemm M,N,K (three untimed launches, ten timed);
+    `props` the mixture-property kernel on --cells cells of the 53-species
+    workload (three untimed launches, five timed after a 256 MiB L2 flush)."""
+    import ctypes as C
+    import torch
+    from openhurricane_b200 import _capi, synth, workloads
+    from openhurricane_b200.chemistry import Mechanism
+    dev = torch.device("cuda:0")
+    d = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+    st = torch.cuda.current_stream()
+
+    def timed(fn, reps, flush=None):
+        for _ in range(3):
+            fn()
+        times = []
+        for k in range(reps):
+            if flush is not None:
+                flush.fill_(float(k))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            fn()
+            b.record(st)
+            torch.cuda.synchronize()
+            times.append(a.elapsed_time(b))
+        return float(np.median(times))
+
+    if args.profile == "gemm":
+        from openhurricane_b200.surrogate import gemm_bf16
+        M, N, K = (int(x) for x in args.gemm.split(","))
+        g = torch.Generator(device="cpu").manual_seed(0)
+        A = torch.randn(M, K, generator=g).to(torch.bfloat16).to(dev)
+        B = torch.randn(N, K, generator=g).to(torch.bfloat16).to(dev)
+        ms = timed(lambda: gemm_bf16(A, B), 10)
+        return {"profile": "gemm", "M": M, "N": N, "K": K, "ms": ms,
+                "TFLOPs": 2.0 * M * N * K / (ms * 1e-3) / 1e12}
+    if args.profile == "props":
+        n = args.cells or 262144
+        _, _, t = workloads.mechanism_files("large")
+        c = workloads.large_cells(n, 3003)
+        m = Mechanism(t)
+        T, p, Y = d(c.T), d(c.p), d(c.Y)
+        flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+        ms = timed(lambda: m.properties(T, p, Y), 5, flush)
+        nbytes = n * 8.0 * ((2 + t.nsp) + (2 * t.nsp + 3))
+        return {"profile": "props", "cells": n, "species": t.nsp, "ms": ms,
+                "cells_per_s": n / (ms * 1e-3), "algorithmic_bytes": nbytes,
+                "GB_per_s": nbytes / (ms * 1e-3) / 1e9}
+    # integrate
+    n = args.cells or 4096
+    name = args.workload
+    if name == "batched":
+        wl = workloads.make_batched(max(n, 65536), pool=512)
+        idx = np.linspace(0, wl.n - 1, n).astype(np.int64)
+        T0, p0, r0, Y0, dt = wl.T[idx], wl.p[idx], wl.rho[idx], wl.Y[:, idx], wl.dt
+        t = wl.tables
+    else:
+        _, _, t = workloads.mechanism_files(name)
+        c = workloads.small_cells(n, 1001) if name == "small" else workloads.large_cells(n, 3003)
+        T0, p0, r0, Y0, dt = c.T, c.p, synth.mixture_density(t.W, c), c.Y, args.dt
+    m = Mechanism(t)
+    if args.kernel is not None:
+        m.set_tuning(args.kernel, args.block)
+    T, p, rho, Y = d(T0), d(p0), d(r0), d(Y0)
+    dtt = torch.full((n,), dt, dtype=torch.float64, device=dev)
+    sub = dtt.clone()
+    o = _capi.default_opts(max_newton_total=args.cap, **workloads.SOLVER_OPTS)
+    vp = lambda x: C.c_void_p(x.data_ptr())
+    cnt = _capi.HcCounters()
+    t0 = time.perf_counter()
+    rc = _capi.load().hc_integrate(m.handle, C.byref(o), n, vp(T), vp(p), vp(rho), vp(Y), vp(dtt),
+                                   1.0, vp(sub), None, None, C.addressof(cnt),
+                                   C.c_void_p(st.cuda_stream))
+    _capi.check(rc, "hc_integrate")
+    torch.cuda.synchronize()
+    secs = time.perf_counter() - t0
+    return {"profile": "integrate", "workload": name, "cells": n, "cap": args.cap,
+            "kernel": args.kernel, "seconds": secs, "newton": int(cnt.n_newton),
+            "newton_per_s": cnt.n_newton / secs}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -532,6 +667,11 @@ def main():
     ap.add_argument("--kernel", type=int, default=None, help="0 auto, 1 thread/cell, 2 group")
     ap.add_argument("--block", type=int, default=64)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--graph", type=int, default=1,
+                    help="1: time each step as a replay of the captured flow step (CUDA graph)")
+    ap.add_argument("--budget-s", type=float, default=1500.0,
+                    help="wall-clock budget of the run: legs after the timed steps that would "
+                         "overrun it are skipped (the timed steps never are)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--prop-cells", type=int, default=262144,
@@ -540,7 +680,15 @@ def main():
                     help="1: also train and time the gated surrogate (batched workload)")
     ap.add_argument("--sur-samples", type=int, default=524288)
     ap.add_argument("--sur-epochs", type=int, default=150)
+    ap.add_argument("--profile", choices=["integrate", "gemm", "props"], default=None,
+                    help="run one small profiling case instead of the benchmark")
+    ap.add_argument("--cap", type=int, default=0, help="--profile integrate: Newton cap per cell")
+    ap.add_argument("--dt", type=float, default=1e-6, help="--profile integrate: dt (small / large)")
+    ap.add_argument("--gemm", default="8192,256,256", help="--profile gemm: M,N,K")
     args = ap.parse_args()
+    if args.profile:
+        print(json.dumps(run_profile(args)), flush=True)
+        return
     if args.warmup < 1:
         raise SystemExit("--warmup must be >= 1")
     ws, rank, local = _dist()

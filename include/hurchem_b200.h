@@ -190,12 +190,18 @@ void hc_default_opts(hc_opts *opts);
  * 5 = thread per cell generated for this mechanism with the Newton matrix
  * I - dt J assembled column by column from register-held rates and written
  * once per entry, no divisions on the common path and a small instruction
- * footprint (NVRTC on first use, like 3);
- * block = threads per block of the thread-per-cell kernels (32, 64 or 128). Set by the autotuner (openhurricane_b200/autotune.py).
+ * footprint (NVRTC on first use, like 3), 6 = warp per cell (one cell per
+ * warp, lane i holding element i and row i of the Newton matrix; nsp + 1 <= 16),
+ * 7 = segment per cell (32 / (nsp + 1) cells per warp, one per segment of
+ * nsp + 1 lanes, each segment with its own step-control state; nsp + 1 <= 16);
+ * block = threads per block of the thread-per-cell kernels (32, 64 or 128;
+ * kernels 6 and 7 run 256-thread blocks whatever it says). Set by the
+ * autotuner (openhurricane_b200/autotune.py).
  * The thread-per-cell kernels (1, 3, 4, 5) take nsp <= 15, the constant-pressure
  * reactor and the common rate forms (Arrhenius, third body, Lindemann / Troe
  * fall-off); a call that asks for one of them outside that range fails with
- * HC_E_UNSUPPORTED. The cell group takes everything hc_mech_create accepts.
+ * HC_E_UNSUPPORTED; kernels 6 and 7 take the same rate forms and reactor,
+ * and autoUpdateJacobian. The cell group takes everything hc_mech_create accepts.
  * No reference counterpart.
  */
 int hc_set_tuning(hc_mech_t mech, int kernel, int block);
@@ -235,6 +241,10 @@ int hc_mech_nrc(hc_mech_t mech);
  *   Ri[nsp*ncells]   optional out (may be NULL): (c_new - c_old)/(dt*dt_factor)*W_i
  *   status[ncells]   optional out: HC_CELL_* bits
  *   counters         optional out (host struct; forces a stream sync)
+ * The device work queue and the counters live in the mechanism (one set per
+ * hc_mech_t): calls of hc_integrate* on the same mechanism that overlap in
+ * time on different streams race on them, so callers that integrate on
+ * several streams at once create one hc_mech_t per stream.
  */
 int hc_integrate(hc_mech_t mech, const hc_opts *opts, int64_t ncells, double *T, const double *p,
                  double *rho, double *Y, const double *dt, double dt_factor, double *subdt,
@@ -281,9 +291,15 @@ int hc_integrate_subset(hc_mech_t mech, const hc_opts *opts, int64_t ncells, int
  * this call allocates nothing: its scratch is a fixed file-scope device array
  * for at most HC_NOALLOC_MAX_CELLS cells (16 MiB, part of the library's
  * device image, placed in device memory when the CUDA runtime loads that
- * image), and larger calls are rejected with HC_E_INVALID. The first call on each device looks up that
- * array's address (cudaGetSymbolAddress, with that device current); make it
- * before any stream capture. The work queue in the array is zeroed with
+ * image), and larger calls are rejected with HC_E_INVALID. Every call made
+ * outside a stream capture looks up that array's address on the current
+ * device (cudaGetSymbolAddress; after a cudaDeviceReset the next call finds
+ * the array's new place); a call under capture uses the address of the last
+ * lookup on that device, so make one call on each device before capturing
+ * (the first may also load the library's device image under lazy module
+ * loading). The kernel is always the compact thread-per-cell kernel
+ * (hc_set_tuning kernel 4): the kernel chosen with hc_set_tuning is not
+ * consulted, only its block size applies. The work queue in the array is zeroed with
  * cudaMemsetAsync at every call. All calls share the array: calls that
  * overlap in time (other streams, other host threads) race on it, so callers
  * serialise them. Returns HC_OK or a negative HC_E_* code; per-cell statuses

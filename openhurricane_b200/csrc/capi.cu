@@ -290,10 +290,14 @@ static bool pack_t2(const HostMech &h, const hc_mech_desc *d, T2Mech &t) {
     return true;
 }
 
-// The mechanism in the warp-per-cell kernel's tables (wcell.cuh): species
-// NASA-7 pre-multiplied by W and the polynomial factors, reactions in the
-// mechanism's own order (the order the reference sums f and J in), each
-// species' participation list, the third-body / fall-off reactions.
+// The mechanism in the warp- and segment-per-cell kernels' tables
+// (wcell.cuh, scell.cuh): species NASA-7 pre-multiplied by W and the
+// polynomial factors; reactions in table slots grouped by rate form (plain
+// Arrhenius, third body, fall-off; mechanism order within each group), so
+// that the lanes evaluating one round of slots mostly take the same branch;
+// each species' participation list in the mechanism's own order (the order
+// the reference sums f and J in), naming slots; the third-body / fall-off
+// reactions in mechanism order.
 struct WHost {
     std::vector<double> th, rd, eff, raw, lnu, xj;
     std::vector<int32_t> ri, lptr, lent, tbl;
@@ -330,17 +334,28 @@ static bool pack_w(const HostMech &h, WHost &w) {
     }
     std::vector<int> dev(nrc);   // mechanism order -> device order
     for (int r = 0; r < nrc; ++r) dev[((int)h.perm.size() == nrc) ? h.perm[r] : r] = r;
+    std::vector<int> slot(nrc);  // mechanism order -> table slot
+    {
+        auto cls = [&](int o) {
+            const int t = h.rate_type[dev[o]];
+            return (t == HC_RATE_ARRHENIUS) ? 0 : (t == HC_RATE_THIRD_BODY) ? 1 : 2;
+        };
+        int q = 0;
+        for (int c = 0; c < 3; ++c)
+            for (int o = 0; o < nrc; ++o)
+                if (cls(o) == c) slot[o] = q++;
+    }
     w.rd.assign((size_t)kWRDn * n32, 0.0);
     w.ri.assign((size_t)kWRIn * n32, 0);
     w.eff.assign((size_t)std::max(nrc, 1) * nsp, 0.0);
     double worst = 1.0;
     for (int o = 0; o < nrc; ++o) {
-        const int r = dev[o];
+        const int r = dev[o], q = slot[o];
         const int type = h.rate_type[r], nf = h.nf[r], nb = h.nb[r];
         if (nf + nb > 8) return false;
         // round-major: [round][field][32]
-        auto RI = [&](int f) -> int32_t & { return w.ri[((size_t)(o >> 5) * kWRIn + f) * 32 + (o & 31)]; };
-        auto RD = [&](int f) -> double & { return w.rd[((size_t)(o >> 5) * kWRDn + f) * 32 + (o & 31)]; };
+        auto RI = [&](int f) -> int32_t & { return w.ri[((size_t)(q >> 5) * kWRIn + f) * 32 + (q & 31)]; };
+        auto RD = [&](int f) -> double & { return w.rd[((size_t)(q >> 5) * kWRDn + f) * 32 + (q & 31)]; };
         RI(kWtype) = type;
         RI(kWrev) = h.reversible[r] ? 1 : 0;
         RI(kWnf) = nf;
@@ -376,8 +391,8 @@ static bool pack_w(const HostMech &h, WHost &w) {
         for (int k = nf + nb; k < 8; ++k) RD(kWord + k) = 1.0;
         if (h.reversible[r]) worst = std::max(worst, sn);
         if (type != HC_RATE_ARRHENIUS) {
-            for (int i = 0; i < nsp; ++i) w.eff[(size_t)o * nsp + i] = h.eff[(size_t)r * nsp + i];
-            w.tbl.push_back(o);
+            for (int i = 0; i < nsp; ++i) w.eff[(size_t)q * nsp + i] = h.eff[(size_t)r * nsp + i];
+            w.tbl.push_back(q);
         }
     }
     // participation lists: per entry the reaction, the species' position
@@ -389,12 +404,12 @@ static bool pack_w(const HostMech &h, WHost &w) {
         std::vector<std::array<double, 3>> jobs(nrc);
         for (int o = 0; o < nrc; ++o) {
             const int r = dev[o];
-            jobs[o] = {h.arr[3 * r + 1], -h.arr[3 * r + 2], 0.0};
+            jobs[slot[o]] = {h.arr[3 * r + 1], -h.arr[3 * r + 2], 0.0};
         }
         for (int o = 0; o < nrc; ++o) {
-            const int r = dev[o], type = h.rate_type[r];
+            const int r = dev[o], type = h.rate_type[r], q = slot[o];
             if (type < HC_RATE_LINDEMANN) continue;
-            w.ri[((size_t)(o >> 5) * kWRIn + kWxj) * 32 + (o & 31)] = (int32_t)jobs.size();
+            w.ri[((size_t)(q >> 5) * kWRIn + kWxj) * 32 + (q & 31)] = (int32_t)jobs.size();
             jobs.push_back({h.arr0[3 * r + 1], -h.arr0[3 * r + 2], 0.0});
             if (type == HC_RATE_TROE3 || type == HC_RATE_TROE4) {
                 jobs.push_back({0.0, 0.0, -1.0 / h.troe[4 * r + 1]});
@@ -414,14 +429,15 @@ static bool pack_w(const HostMech &h, WHost &w) {
     for (int i = 0; i < nsp; ++i) {
         w.lptr[i] = (int32_t)w.lnu.size();
         for (int o = 0; o < nrc; ++o) {
-            auto RI = [&](int f) { return w.ri[((size_t)(o >> 5) * kWRIn + f) * 32 + (o & 31)]; };
-            auto RD = [&](int f) { return w.rd[((size_t)(o >> 5) * kWRDn + f) * 32 + (o & 31)]; };
+            const int q = slot[o];
+            auto RI = [&](int f) { return w.ri[((size_t)(q >> 5) * kWRIn + f) * 32 + (q & 31)]; };
+            auto RD = [&](int f) { return w.rd[((size_t)(q >> 5) * kWRDn + f) * 32 + (q & 31)]; };
             const int np = RI(kWnf) + RI(kWnb);
             uint32_t c[2] = {0u, 0u};
             for (int k = 0; k < np; ++k) c[k >> 2] |= (uint32_t)RI(kWidx + k) << (8 * (k & 3));
             for (int k = 0; k < np; ++k) {
                 if (RI(kWidx + k) != i) continue;
-                w.lent.push_back(o | (k << 16) | (np << 20) | ((RI(kWtype) != HC_RATE_ARRHENIUS) ? (1 << 24) : 0));
+                w.lent.push_back(q | (k << 16) | (np << 20) | ((RI(kWtype) != HC_RATE_ARRHENIUS) ? (1 << 24) : 0));
                 w.lent.push_back((int32_t)c[0]);
                 w.lent.push_back((int32_t)c[1]);
                 w.lnu.push_back(RD(kWnu + k));
@@ -700,7 +716,7 @@ int hc_mech_create(const hc_mech_desc *d, hc_mech_t *out) {
 
 int hc_set_tuning(hc_mech_t m, int kernel, int block) {
     if (!m) return fail(HC_E_INVALID, "null mechanism");
-    if (kernel < 0 || kernel > 6) return fail(HC_E_INVALID, "kernel must be 0 .. 6");
+    if (kernel < 0 || kernel > 7) return fail(HC_E_INVALID, "kernel must be 0 .. 7");
     if (block != 32 && block != 64 && block != 128)
         return fail(HC_E_INVALID, "block must be 32, 64 or 128");
     if (block != m->block) {
@@ -840,6 +856,13 @@ static int integrate_impl(hc_mech_t m, const hc_opts *opts, int64_t ncells, doub
             m->ylast_cells = (size_t)ncells;
         }
         return variant_integrate_t2(N, m->t2, m->num_sms, P, io, m->ylast, m->block, st, g_err);
+    }
+    if (m->kernel == 7) {
+        if (!m->w_ok || opts->reactor != 0)
+            return fail(HC_E_UNSUPPORTED,
+                        "segment-per-cell kernel needs nsp + 1 <= 16, the constant-pressure reactor and no "
+                        "SRI, explicit reverse (REV), PLOG, HIGH, LT, JAN, FIT1 or collision rate laws");
+        return launch_integrate_s(m->w, m->num_sms, P, io, st, g_err);
     }
     if (m->kernel == 6) {
         if (!m->w_ok || opts->reactor != 0)
@@ -1736,7 +1759,7 @@ constexpr size_t kNoAllocYlast = 2 * 16 * (size_t)HC_NOALLOC_MAX_CELLS;   // dou
 __device__ __align__(256) double g_noalloc_scratch[kNoAllocYlast + 8];
 
 std::mutex g_noalloc_mu;
-void *g_noalloc_addr[256] = {};   // the array's device address, per device
+void *g_noalloc_addr[256] = {};   // the array's device address at the last lookup, per device
 
 }  // namespace
 
@@ -1764,18 +1787,23 @@ extern "C" int hc_integrate_noalloc(hc_mech_t m, const hc_opts *opts, int64_t nc
     int dev = -1;
     HC_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 256) return fail(HC_E_CUDA, "device ordinal out of range");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
     void *base = nullptr;
     {
-        // the array's address is looked up once per device, with that device current
+        // the array's address: looked up at every call outside a stream
+        // capture (a new context after cudaDeviceReset places the array
+        // anew), and taken from the last lookup on this device during a
+        // capture (no context can be reset while one is open)
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        HC_CUDA(cudaStreamIsCapturing(st, &cs));
         std::lock_guard<std::mutex> lk(g_noalloc_mu);
-        if (!g_noalloc_addr[dev]) {
+        if (cs == cudaStreamCaptureStatusNone || !g_noalloc_addr[dev]) {
             void *a = nullptr;
             HC_CUDA(cudaGetSymbolAddress(&a, g_noalloc_scratch));
             g_noalloc_addr[dev] = a;
         }
         base = g_noalloc_addr[dev];
     }
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     double *ylast = static_cast<double *>(base);
     unsigned long long *queue = reinterpret_cast<unsigned long long *>(ylast + kNoAllocYlast);
     HC_CUDA(cudaMemsetAsync(queue, 0, 8 * sizeof(unsigned long long), st));

@@ -39,6 +39,8 @@ struct WMech;
 // the warp-per-cell integrator (variant_w.cu, wcell.cuh)
 int launch_integrate_w(const WMech &m, int num_sms, const IntegratorParams &P, const CellIO &io,
                        cudaStream_t st, std::string &err);
+int launch_integrate_s(const WMech &m, int num_sms, const IntegratorParams &P, const CellIO &io,
+                       cudaStream_t st, std::string &err);
 int launch_properties(const DevMech &m, int64_t n, const double *T, const double *p,
                       const double *Y, double *ha, double *cp, double *mu, double *kappa,
                       double *D, cudaStream_t st, std::string &err);

@@ -10,7 +10,8 @@ import tempfile
 import numpy as np
 import pytest
 
-EXAMPLE = "/root/reference/example/ObliqueDetonation"
+# the reference tree: HC_REFERENCE, else the Makefile's default (oracle/Makefile.ref)
+EXAMPLE = os.path.join(os.environ.get("HC_REFERENCE", "/root/reference"), "example", "ObliqueDetonation")
 
 
 def _files():

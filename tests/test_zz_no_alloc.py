@@ -98,3 +98,52 @@ def test_noalloc_rejects_more_cells_than_its_scratch(small):
                                   vp(x), vp(Y), vp(x), 1.0, vp(x), None, None, None)
     assert rc == -1
     assert b"HC_NOALLOC_MAX_CELLS" in lib.hc_last_error()
+
+
+def test_noalloc_replays_from_a_cuda_graph(small):
+    """One eager call (looks the scratch array up), then the same call
+    captured in a CUDA graph and replayed on restored inputs: bit-identical
+    to the eager result, with no change of free device memory on replay."""
+    from openhurricane_b200 import _capi, workloads
+    from openhurricane_b200.chemistry import Mechanism
+    dev = _dev()
+    t = small["tables"]
+    mech = Mechanism(t)
+    mech.set_tuning(4, 64)
+    n = 2048
+    T0, p0, r0, Y0 = (torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+                      for a in _cells(t, n, seed=616))
+    opts = _capi.default_opts(**workloads.SOLVER_OPTS)
+    eager = _run("noalloc", mech, opts, (T0, p0, r0, Y0), n, 1e-6)
+    T, rho, Y = T0.clone(), r0.clone(), Y0.clone()
+    dtt = torch.full((n,), 1e-6, dtype=torch.float64, device=dev)
+    sub = dtt.clone()
+    st = torch.zeros(n, dtype=torch.int32, device=dev)
+    vp = lambda x: C.c_void_p(x.data_ptr())
+    lib = _capi.load()
+    g = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        with torch.cuda.graph(g, stream=side):
+            rc = lib.hc_integrate_noalloc(mech.handle, C.byref(opts), n, vp(T), vp(p0), vp(rho), vp(Y),
+                                          vp(dtt), 1.0, vp(sub), None, vp(st),
+                                          C.c_void_p(side.cuda_stream))
+            assert rc == 0, lib.hc_last_error()
+    torch.cuda.current_stream().wait_stream(side)
+    # capture recorded the work without running it: restore and replay
+    T.copy_(T0)
+    rho.copy_(r0)
+    Y.copy_(Y0)
+    sub.fill_(1e-6)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    g.replay()
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert np.array_equal(T.cpu().numpy(), eager[0])
+    assert np.array_equal(rho.cpu().numpy(), eager[1])
+    assert np.array_equal(Y.cpu().numpy(), eager[2])
+    assert np.array_equal(st.cpu().numpy(), eager[4])
+    assert free1 == free0
+    del g
