@@ -27,6 +27,13 @@ and stores inputs and outputs:
                   of its cells answer one-ulp input changes with 1e-6 changes
                   of T); plus KAT states,
                   point-implicit source terms and properties of 16 cells.
+  batched_ref.npz: the benchmarked configuration: 256 cells strided from
+                  the 1,048,576 cells of the batched workload (seed 2002; 20 %
+                  ignition, 80 % near equilibrium), dt = 1e-5 s, the
+                  benchmark's solver options (atol 1e-11, rtol 1e-4, maxstep
+                  10000); integration outputs only.
+  large32_ref.npz: 32 cells of the 53-species mechanism drawn like the large
+                  workload, dt = 1e-6 s, atol 1e-15; integration outputs only.
   fitted_ref.npz: the small mechanism with Janev (JAN), power-series (FIT1),
                   reverse Landau-Teller (LT + REV + RLT) and collision-
                   efficiency (COLLEFF) reactions (synth.fitted_rates_mechanism),
@@ -38,7 +45,8 @@ The mechanism files are regenerated from their seeds by
 openhurricane_b200.synth at test time; a SHA-256 of the generated text files
 is stored so that a change of the generator is detected.
 
-    python tests/golden/make_golden.py [small] [large] [ext] [cv] [fitted]   (default: all;
+    python tests/golden/make_golden.py [small] [large] [ext] [cv] [fitted] [batched] [large32]
+    (default: all;
     needs oracle/_ref/hurchem_ref)
 """
 import hashlib
@@ -146,10 +154,42 @@ def make_cv(out):
     print("cv written", out)
 
 
+def make_integration(out, mech, T, p, rho, Y, dt, opts):
+    """Integration outputs only, at the given solver options."""
+    work = tempfile.mkdtemp(prefix="golden_int_")
+    files = synth.write_chemkin(mech, work)
+    case = os.path.join(work, "case.cont")
+    refrun.write_case(case, *files, dict(opts))
+    res = refrun.integrate(case, T, p, rho, dt, dt, Y, procs=os.cpu_count() or 1, workdir=work)
+    np.savez_compressed(out, sha=files_sha(files), seed=mech.seed, dt=dt,
+                        opts=np.array(sorted(opts.items()), dtype=object).astype(str),
+                        in_T=T, in_p=p, in_rho=rho, in_Y=Y,
+                        out_T=res["T"], out_Y=res["Y"], out_rho=res["rho"], out_c=res["c"],
+                        out_subdt=res["subdt"], out_status=res["status"])
+    print(os.path.basename(out), "written, reference seconds", res["seconds"])
+
+
 def main():
     if not refrun.available():
         raise SystemExit("oracle/_ref/hurchem_ref is missing: make -f oracle/Makefile.ref")
-    which = set(sys.argv[1:]) or {"small", "large", "ext", "cv", "fitted"}
+    which = set(sys.argv[1:]) or {"small", "large", "ext", "cv", "fitted", "batched", "large32"}
+    if "batched" in which:
+        # the benchmarked configuration: 256 cells strided from the 1,048,576
+        # batched cells (seed 2002), dt = 1e-5 s, the benchmark's solver options
+        from openhurricane_b200 import workloads
+        wl = workloads.make_batched(1048576)
+        idx = np.linspace(0, wl.n - 1, 256).astype(np.int64)
+        make_integration(os.path.join(HERE, "batched_ref.npz"), synth.small_mechanism(),
+                         wl.T[idx], wl.p[idx], wl.rho[idx], np.ascontiguousarray(wl.Y[:, idx]),
+                         wl.dt, workloads.SOLVER_OPTS)
+    if "large32" in which:
+        # 32 cells of the 53-species mechanism drawn like the large workload, dt = 1e-6 s
+        large = synth.large_mechanism()
+        c = synth.dirichlet_cells(53, 32, seed=117, T_range=(800, 2800), p_atm_range=(0.5, 10),
+                                  alpha=0.3)
+        rho = synth.mixture_density(large.weights(), c)
+        make_integration(os.path.join(HERE, "large32_ref.npz"), large, c.T, c.p, rho, c.Y, 1e-6,
+                         {"atol": 1e-15})
     if "small" in which:
         small = synth.small_mechanism()
         make("small", small, synth.dirichlet_cells(9, 48, seed=101), 1e-6, 8,

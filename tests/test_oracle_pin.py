@@ -48,6 +48,24 @@ def test_oracle_integration_bit_exact_vs_reference_golden(name, request):
         assert np.array_equal(o[k], g["out_" + k]), k
 
 
+@pytest.mark.parametrize("name,mech,opts", [
+    ("batched", "small", dict(atol=1e-11, rtol=1e-4)),   # the benchmarked configuration
+    ("large32", "large", dict(atol=1e-15)),
+])
+def test_oracle_integration_bit_exact_vs_reference_golden_at_options(name, mech, opts, request):
+    """The benchmarked cells at the benchmark's solver options and 32 cells of
+    the 53-species mechanism: the oracle reproduces the reference bit for bit."""
+    from oracle import port
+    mk = request.getfixturevalue(mech)
+    g = _load(name)
+    assert _sha(mk["files"]) == str(g["sha"])
+    md = port.MechDesc(mk["tables"])
+    o = port.integrate(md, g["in_T"], g["in_p"], g["in_rho"], g["in_Y"], float(g["dt"]),
+                       opts=port.default_opts(**opts))
+    for k in ("T", "Y", "rho", "c", "subdt"):
+        assert np.array_equal(o[k], g["out_" + k]), k
+
+
 @pytest.mark.parametrize("name", ["small", "large", "ext", "fitted"])
 def test_oracle_kernels_bit_exact_vs_reference_golden(name, request):
     from oracle import port
