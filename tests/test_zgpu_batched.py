@@ -25,16 +25,15 @@ import os
 import numpy as np
 import pytest
 
+from parity_util import check as _check
+from parity_util import oracle as _oracle
+
 torch = pytest.importorskip("torch")
 
 pytestmark = pytest.mark.gpu
 
-T_RTOL = 1e-6
-Y_RTOL = 1e-5
-Y_FLOOR = 1e-12
 PARITY = dict(atol=1e-15, rtol=1e-6)
 BENCH = dict(atol=1e-11, rtol=1e-4)
-MAX_FLIP_FRACTION = 0.05
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -71,68 +70,6 @@ def _gpu(tables, kernel, T, p, rho, Y, dt, **opts):
             "status": st.cpu().numpy()}
 
 
-def _oracle(tables, T, p, rho, Y, dt, **opts):
-    from oracle import port
-    return port.integrate(port.MechDesc(tables), T, p, rho, Y, dt, opts=port.default_opts(**opts))
-
-
-def _bad_cells(g, ref):
-    dT = np.abs(g["T"] - ref["T"]) / np.abs(ref["T"])
-    dr = np.abs(g["rho"] - ref["rho"]) / np.abs(ref["rho"])
-    dY = (np.abs(g["Y"] - ref["Y"]) - Y_RTOL * np.abs(ref["Y"]) - Y_FLOOR).max(axis=0)
-    return np.where((dT > T_RTOL) | (dr > T_RTOL) | (dY > 0.0))[0]
-
-
-def _perturbations(T, Y, k):
-    """Inputs one unit in the last place away: T up / down, all Y up / down,
-    then seeded +-1 ulp patterns over the species and T."""
-    ulp = np.finfo(np.float64).eps
-    if k == 0:
-        return T * (1 + ulp), Y
-    if k == 1:
-        return T * (1 - ulp / 2), Y
-    if k == 2:
-        return T, Y * (1 + ulp)
-    if k == 3:
-        return T, Y * (1 - ulp / 2)
-    rng = np.random.default_rng(k)
-    sT = rng.choice([-0.5, 1.0], size=T.shape)
-    sY = rng.choice([-0.5, 0.0, 1.0], size=Y.shape)
-    return T * (1 + sT * ulp), Y * (1 + sY * ulp)
-
-
-def _explain(tables, inp, g, bad, dt, opts, tries=16):
-    """The cells of `bad` that the oracle reproduces from a one-ulp
-    perturbation of their inputs (within the parity tolerance of the GPU's
-    answer); returns the unexplained ones."""
-    T, p, rho, Y = (a[..., bad] for a in inp)
-    gb = {k: g[k][..., bad] for k in ("T", "rho", "Y")}
-    left = np.arange(bad.size)
-    for k in range(tries):
-        if left.size == 0:
-            break
-        Tk, Yk = _perturbations(T[left], Y[:, left], k)
-        o = _oracle(tables, Tk, p[left], rho[left], Yk, dt, **opts)
-        sub = {key: gb[key][..., left] for key in gb}
-        still = _bad_cells(sub, {"T": o["T"], "rho": o["rho"], "Y": o["Y"]})
-        left = left[still]
-    return bad[left]
-
-
-def _check(tables, inp, g, ref, dt, opts, what):
-    bad = _bad_cells(g, ref)
-    n = inp[0].shape[0]
-    assert bad.size <= MAX_FLIP_FRACTION * n, f"{what}: {bad.size} of {n} cells outside tolerance"
-    unexplained = _explain(tables, inp, g, bad, dt, opts) if bad.size else bad
-    assert unexplained.size == 0, f"{what}: cells {unexplained.tolist()} outside tolerance, unexplained"
-    # the statuses agree where the answers do
-    return bad
-
-
-def _kernels(nsp):
-    return (0, 2, 4, 6, 7) if nsp + 1 <= 16 else (0,)
-
-
 @pytest.mark.parametrize("kernel", [0, 6, 7])
 def test_batched_sample_vs_oracle_tight(small, kernel):
     g0 = _golden("batched")
@@ -156,7 +93,7 @@ def test_batched_sample_vs_reference_golden_at_bench_options(small, kernel):
     _check(t, inp, g, ref, dt, BENCH, f"kernel {kernel}, batched sample vs reference")
 
 
-@pytest.mark.parametrize("kernel", [0, 7])
+@pytest.mark.parametrize("kernel", [0, 6, 7])
 def test_small_configuration_4096_cells_vs_oracle(small, kernel):
     from openhurricane_b200 import synth, workloads
     t = small["tables"]

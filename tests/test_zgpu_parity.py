@@ -135,8 +135,9 @@ def test_large_mechanism_parity_vs_oracle(large, kernel, block):
 
 @pytest.mark.parametrize("name", ["small", "large"])
 def test_against_reference_golden_outputs(name, request):
-    """The reference's own outputs (default rtol 1e-4, atol 1e-15): most cells
-    agree to the parity tolerance and every cell agrees to the solver's rtol."""
+    """The reference's own outputs (default rtol 1e-4, atol 1e-15): every cell
+    agrees to the parity tolerance or is explained (parity_util.check), and
+    every cell agrees to the solver's rtol."""
     mk = request.getfixturevalue(name)
     g0 = _golden(name)
     m = _mech(mk["tables"])
@@ -148,9 +149,12 @@ def test_against_reference_golden_outputs(name, request):
                        atol=1e-15, **cap)
     dT = np.abs(g["T"] - g0["out_T"]) / g0["out_T"]
     assert dT.max() < 1e-4
-    dY = np.abs(g["Y"] - g0["out_Y"]) - Y_RTOL * np.abs(g0["out_Y"]) - Y_FLOOR
-    ok = (dT <= T_RTOL) & (dY.max(axis=0) <= 0.0)
-    assert ok.mean() >= 0.9, f"{ok.mean():.3f} of cells within parity tolerance"
+    # every cell within the parity tolerance, or explained as a threshold
+    # decision taken the other way (one-ulp perturbation of the oracle)
+    from parity_util import check
+    check(mk["tables"], (g0["in_T"], g0["in_p"], g0["in_rho"], g0["in_Y"]), g,
+          {"T": g0["out_T"], "rho": g0["out_rho"], "Y": g0["out_Y"]}, float(g0["dt"]),
+          dict(atol=1e-15, **cap), f"{name} vs reference")
 
 
 @pytest.mark.parametrize("name", ["small", "large"])
