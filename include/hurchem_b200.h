@@ -179,9 +179,10 @@ const char *hc_last_error(void);
 void hc_default_opts(hc_opts *opts);
 
 /*
- * Kernel selection for hc_integrate*: kernel 0 = automatic (the cell group:
- * its lanes share each Newton iteration of one cell, which bounds the step's
- * duration when per-cell costs are uneven), 1 = table-driven thread per
+ * Kernel selection for hc_integrate*: kernel 0 = automatic (the warp per
+ * cell, kernel 6, wherever it takes the mechanism and the reactor, else the
+ * cell group: their lanes share each Newton iteration of one cell, which
+ * bounds the step's duration when per-cell costs are uneven), 1 = table-driven thread per
  * cell, 2 = cell group (32 lanes up to 32 unknowns, 64 above),
  * 3 = thread per cell generated for this mechanism (every index and
  * coefficient a literal; compiled with NVRTC for sm_100a on first use, which

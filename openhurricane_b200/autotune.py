@@ -1,6 +1,8 @@
 """Autotuner for the integrator's launch shape.
 
 Candidates are (kernel, block) pairs accepted by hc_set_tuning:
+kernel 6 = warp per cell, kernel 7 = segment per cell (nsp + 1 <= 16;
+256-thread blocks, the block argument is unused),
 kernel 1 = thread per cell (nsp + 1 <= 16; block 32/64/128 threads),
 kernel 3 = thread per cell generated for the mechanism (same limits),
 kernel 4 = compact thread per cell (mechanism in the constant bank),
@@ -30,7 +32,9 @@ _MEMO: Dict[str, dict] = {}
 def candidates(nsp: int) -> List[Tuple[int, int]]:
     c = []
     if nsp + 1 <= 16:
-        c += [(4, 32), (4, 64), (4, 128), (3, 64), (1, 64)]
+        # warp and segment per cell (256-thread blocks: block unused), then
+        # the thread-per-cell kernels
+        c += [(6, 64), (7, 64), (4, 64), (4, 128), (3, 64), (1, 64)]
     c += [(2, 64)]      # the cell group's width is fixed by the variant; block is unused
     return c
 

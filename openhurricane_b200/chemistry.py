@@ -58,7 +58,8 @@ class Mechanism:
         return cls(compile_mechanism(che, thermo, transport))
 
     def set_tuning(self, kernel: int = 0, block: int = 64):
-        """kernel: 0 automatic (cell group), 1 table-driven thread per cell, 2 cell group,
+        """kernel: 0 automatic (warp per cell where it applies, else the cell group),
+        1 table-driven thread per cell, 2 cell group,
         3 generated thread per cell, 4 compact thread per cell, 5 generated direct-assembly
         thread per cell, 6 warp per cell, 7 segment per cell (see hc_set_tuning)."""
         _capi.check(_capi.load().hc_set_tuning(self.handle, int(kernel), int(block)),

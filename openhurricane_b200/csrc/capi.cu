@@ -837,12 +837,10 @@ static int integrate_impl(hc_mech_t m, const hc_opts *opts, int64_t ncells, doub
                     "compact thread-per-cell kernel needs nsp <= 15, <= 64 reactions, "
                     "autoUpdateJacobian off, the constant-pressure reactor and no SRI, explicit "
                     "reverse (REV), PLOG, HIGH, LT, JAN, FIT1 or collision rate laws");
-    // automatic choice: the cell group. Per-cell costs in a flow step differ
-    // by orders of magnitude, and the step lasts as long as its stiffest
-    // cell; the cell group's lanes share each Newton iteration's work and
-    // finish a single cell several times sooner than one thread does, which
-    // outweighs the thread-per-cell kernels' higher throughput on uniform
-    // cells (measured on the batched workload).
+    // Per-cell costs in a flow step differ by orders of magnitude, and the
+    // step lasts as long as its stiffest cell: the cooperative kernels (cell
+    // group, warp per cell) share each Newton iteration of one cell among
+    // lanes and finish a single cell several times sooner than one thread does.
     const bool use_t2 = t1_ok && m->t2_ok && m->kernel == 4;
     if (use_t2) {
         if (m->ylast_cells < (size_t)ncells) {
@@ -864,7 +862,11 @@ static int integrate_impl(hc_mech_t m, const hc_opts *opts, int64_t ncells, doub
                         "SRI, explicit reverse (REV), PLOG, HIGH, LT, JAN, FIT1 or collision rate laws");
         return launch_integrate_s(m->w, m->num_sms, P, io, st, g_err);
     }
-    if (m->kernel == 6) {
+    // automatic choice (kernel 0): the warp-per-cell kernel wherever it takes
+    // the mechanism (the fastest on the batched workload: 1.14e8 Newton
+    // iterations/s against 0.6e8 for the cell group), else the cell group
+    const bool auto_w = m->kernel == 0 && m->w_ok && opts->reactor == 0;
+    if (m->kernel == 6 || auto_w) {
         if (!m->w_ok || opts->reactor != 0)
             return fail(HC_E_UNSUPPORTED,
                         "warp-per-cell kernel needs nsp + 1 <= 16, the constant-pressure reactor and no "

@@ -68,9 +68,8 @@ struct SLayout {
     static constexpr int G = 32 / N;                 // cells per warp
     static constexpr int LD = (N % 2 == 0) ? N + 1 : N;
     static constexpr int kSV = 0;                    // c, h, E, R, g, dgt: 6 x S
-    static constexpr int kJ = 6 * S;                 // rows of J, then of its LU factors: N x LD
-    static constexpr int kP = kJ + N * LD;           // LU: the lane of each logical row (N ints)
-    static constexpr int kRec = kP + (N + 1) / 2;    // records [kWRec][nrc], then the exponentials [njob]
+    static constexpr int kJ = 6 * S;                 // rows of J, N x LD
+    static constexpr int kRec = kJ + N * LD;         // records [kWRec][nrc], then the exponentials [njob]
     __host__ __device__ static size_t doubles(int nrc, int njob) {
         return (size_t)kRec + kWRec * (size_t)(nrc > 0 ? nrc : 1) + (njob > 0 ? njob : 1);
     }
@@ -145,10 +144,9 @@ struct SCtx {
     __device__ __forceinline__ const double *rdp(int r) const { return tb.rd + (r >> 5) * (kWRDn * 32) + (r & 31); }
     __device__ __forceinline__ const int32_t *rip(int r) const { return tb.ri + (r >> 5) * (kWRIn * 32) + (r & 31); }
 
-    // f(y) and, when jac, the Jacobian: the rows go to shared memory in the
-    // segments with jw set (the others keep their LU factors there). Called
-    // by the whole warp; y is this lane's element.
-    __device__ __forceinline__ double evaluate(double y, bool jac, bool jw) {
+    // f(y) and, when jac, the Jacobian rows into shared memory. Called by the
+    // whole warp; y is this lane's element.
+    __device__ __forceinline__ double evaluate(double y, bool jac) {
         const unsigned full = 0xffffffffu;
         const int sl = L.sl;
         const bool act = L.act;
@@ -213,8 +211,7 @@ struct SCtx {
         double *Jrow = s + SL::kJ + sl * SL::LD;
         // rows of the species and of padding species between them and T
         // (zero rows: identity rows of I - dt J)
-        jw = jw && jac && act;
-        if (jw && sl < N - 1) {
+        if (jac && act && sl < N - 1) {
 #pragma unroll
             for (int j = 0; j < N; ++j) Jrow[j] = 0.0;
         }
@@ -231,7 +228,6 @@ struct SCtx {
                 jt += nu * R[rs];
                 Sx += R[3 * rs] * R[(4 + pos) * rs];
                 const unsigned c0 = (unsigned)tb.lent[3 * e + 1], c1 = (unsigned)tb.lent[3 * e + 2];
-                if (!jw) continue;
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
                     if (k >= np) break;
@@ -261,11 +257,11 @@ struct SCtx {
         if (act && sl == TI) f = -DTdt;
         if (jac) {
             const double cpf = L.sum(sp ? cp * f + h * jt : 0.0, full);
-            if (jw && sl < N - 1) {
+            if (act && sl < N - 1) {
                 Jrow[TI] = jt;
                 s[SL::kJ + TI * SL::LD + sl] = sp ? (cp * DTdt - Sx) * icCp : 0.0;
             }
-            if (jw && sl == TI) Jrow[TI] = (dcCpdT * DTdt - cpf) * icCp;
+            if (act && sl == TI) Jrow[TI] = (dcCpdT * DTdt - cpf) * icCp;
         }
         __syncwarp();
         return f;
@@ -402,8 +398,7 @@ struct SCtx {
                 dp[k] = 1.0;
                 if (k < n) {
                     const double o = x[(kWord + off + k) * 32];
-                    if (o == 2.0) dp[k] = 2.0 * hmax(sv[xi[(kWidx + off + k) * 32]], 0.0);
-                    else if (o != 1.0) dp[k] = s_dconc(sv[xi[(kWidx + off + k) * 32]], o);
+                    if (o != 1.0) dp[k] = s_dconc(sv[xi[(kWidx + off + k) * 32]], o);
                 }
             }
 #pragma unroll
@@ -479,39 +474,34 @@ struct SCtx {
                 }
             }
         }
-        // the factors replace J in shared memory, with the lane of each logical row
-        if (fac && act) {
-            double *Lrow = s + SL::kJ + sl * SL::LD;
-#pragma unroll
-            for (int j = 0; j < N; ++j) Lrow[j] = a[j];
-            reinterpret_cast<int *>(s + SL::kP)[lpos] = sl;
-        }
-        __syncwarp();
     }
 
     // (L U) x = P b along the logical order; b and x are this lane's
-    // elements; the factors and the row permutation come from shared memory
-    // (the segment's last factorisation). Called by the whole warp.
+    // elements. Called by the whole warp.
     __device__ __forceinline__ double solve(double b) {
         const unsigned full = 0xffffffffu;
         const int sl = L.sl;
         const bool act = L.act;
-        const double *Lrow = s + SL::kJ + sl * SL::LD;
-        const int *P = reinterpret_cast<const int *>(s + SL::kP);
-        double acc = 0.0, z = 0.0;
-#pragma unroll 1
+        int src[N];
+#pragma unroll
         for (int t = 0; t < N; ++t) {
-            const double zt = __shfl_sync(full, b - acc, (L.base + P[t]) & 31);
+            const unsigned bt = (__ballot_sync(full, act && lpos == t) & L.bits) >> (L.base & 31);
+            src[t] = (L.base + __ffs(bt) - 1) & 31;
+        }
+        double acc = 0.0, z = 0.0;
+#pragma unroll
+        for (int t = 0; t < N; ++t) {
+            const double zt = __shfl_sync(full, b - acc, src[t]);
             if (lpos == t) z = zt;
-            if (act && lpos > t) acc += Lrow[t] * zt;
+            if (act && lpos > t) acc += a[t] * zt;
         }
         double x = 0.0;
         acc = 0.0;
-#pragma unroll 1
+#pragma unroll
         for (int t = N - 1; t >= 0; --t) {
-            const double xt = __shfl_sync(full, (z - acc) * Lrow[t], (L.base + P[t]) & 31);
+            const double xt = __shfl_sync(full, (z - acc) * a[t], src[t]);
             if (sl == t) x = xt;
-            if (act && lpos < t) acc += Lrow[t] * xt;
+            if (act && lpos < t) acc += a[t] * xt;
         }
         return act ? x : 0.0;
     }
@@ -520,10 +510,7 @@ struct SCtx {
 #ifndef HC_S_MIN_BLOCKS
 #define HC_S_MIN_BLOCKS 2   // blocks of kSWarps warps per SM the kernel is built for
 #endif
-#ifndef HC_S_WARPS
-#define HC_S_WARPS 8        // warps per block
-#endif
-constexpr int kSWarps = HC_S_WARPS;
+constexpr int kSWarps = 8;  // warps per block
 
 template <int N>
 __global__ void __launch_bounds__(32 * kSWarps, HC_S_MIN_BLOCKS)
@@ -758,7 +745,7 @@ integrate_s_kernel(const __grid_constant__ WMech m, const __grid_constant__ Inte
         const bool newton = state == kT1Newton;
         const bool fac = newton && jacNow;
         const bool anyJ = __ballot_sync(full, fac) != 0u;
-        const double f = cx.evaluate(yk, anyJ, fac);
+        const double f = cx.evaluate(yk, anyJ);
         if (anyJ) cx.factor(lts0, fac);
         double x = 0.0;
         if (__ballot_sync(full, newton) != 0u) x = cx.solve(L.act ? ((-yk + y) + lts0 * f) : 0.0);

@@ -106,9 +106,6 @@ __host__ __device__ inline size_t w_tables_bytes(int nsp, int nrc, int nrc32, in
     return sizeof(double) * d + ((sizeof(int32_t) * i + 7) & ~(size_t)7);
 }
 
-template <int N>
-__device__ __noinline__ double w_evaluate(const WMech &m, const WTabs &tb, const IntegratorParams &P, double *s,
-                                          int lane, double y, bool jac);
 
 template <int N>
 struct WCtx {
@@ -153,7 +150,7 @@ struct WCtx {
     // temperature row and column). y is this lane's element (lane < N).
     __device__ __forceinline__ double evaluate(double y, bool jac) {
         if (jac) ++n_jac; else ++n_rhs;
-        return w_evaluate<N>(m, tb, P, s, lane, y, jac);
+        return eval_impl(y, jac);
     }
 
     __device__ __forceinline__ double eval_impl(double y, bool jac) {
@@ -203,13 +200,11 @@ struct WCtx {
         // ---- reactions: one record each
         // every exponential of the reaction pass, one per lane
         double *X = s + SM::kRec + kWRec * m.nrc32;
-#pragma unroll 1
         for (int j = lane; j < m.njob; j += 32) {
             const double *xj = tb.xj + (j >> 5) * 96 + (j & 31);
             X[j] = exp(xj[0] * logT + xj[32] * invT + xj[64] * T);
         }
         __syncwarp();
-#pragma unroll 1
         for (int r = lane; r < m.nrc32; r += 32) {
             if (r < m.nrc) reaction(r, T, logT, invT, invRuT, wslow, jac, recp(r), X);
         }
@@ -225,7 +220,6 @@ struct WCtx {
         }
         if (lane < nsp) {
             const int e0 = tb.lptr[lane], e1 = tb.lptr[lane + 1];
-#pragma unroll 1
             for (int e = e0; e < e1; ++e) {
                 const int w0 = tb.lent[3 * e];
                 const int r = w0 & 0xffff, pos = (w0 >> 16) & 7, np = (w0 >> 20) & 15;
@@ -245,13 +239,11 @@ struct WCtx {
                 if (w0 & (1 << 24)) {
                     const double gn = nu * R[2 * 32];
                     const double *er = &tb.eff[(size_t)r * nsp];
-#pragma unroll 1
                     for (int j = 0; j < nsp; ++j) Jrow[j] += er[j] * gn;
                 }
             }
             if (jac) {
                 // the temperature row's third-body / fall-off columns
-#pragma unroll 1
                 for (int t = 0; t < m.ntb; ++t) {
                     const int r = tb.tbl[t];
                     const double *R = recp(r);
@@ -294,7 +286,6 @@ struct WCtx {
         double M = 0.0;
         if (type != kArrhenius) {
             const double *er = &tb.eff[(size_t)r * nsp];
-#pragma unroll 1
             for (int j = 0; j < nsp; ++j) M += er[j] * sv[j];
         }
         const double b = x[(kWb) * 32], Ta = x[(kWTa) * 32];
@@ -492,15 +483,6 @@ struct WCtx {
         return (lane < N) ? x : 0.0;
     }
 };
-
-// One evaluation of f (and J) out of line: the step control calls it from
-// three places, and one copy keeps the kernel inside the instruction cache.
-template <int N>
-__device__ __noinline__ double w_evaluate(const WMech &m, const WTabs &tb, const IntegratorParams &P, double *s,
-                                          int lane, double y, bool jac) {
-    WCtx<N> c(m, tb, P, s, lane);
-    return c.eval_impl(y, jac);
-}
 
 // The reference's step control around WCtx (ImplicitEuler::solve /
 // adaptiveSolve / NewtonIteration, ODEsSolver::maxError; the same control flow
