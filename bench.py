@@ -6,9 +6,17 @@
 A step is one flow step of the chemistry source: every cell of the workload
 is integrated over dt by the FP64 implicit-Euler integrator (one persistent
 work-queue launch, cells ordered stiffest-first by the previous step's
-Newton counts). Each step starts from the same seeded inputs, restored from a
-pristine device copy and followed by an L2 flush (a 256 MiB write) outside
-the per-step CUDA-event window.
+Newton counts), timed as one replay of the captured flow step (CUDA graph:
+queue reset, integrator launch, re-ordering). Each step starts from the same
+seeded inputs, restored from a pristine device copy and followed by an L2
+flush (a 256 MiB write) outside the per-step CUDA-event window. The kernel
+is picked by the autotuner (openhurricane_b200/autotune.py) on a strided
+sample of the workload's cells unless --kernel names one.
+
+The timed steps are exactly --steps; the legs after them (end to end, the
+CPU baseline, the gated surrogate: fixed sizes, 3 timed steps whatever
+--steps says) run within --budget-s of wall-clock time, and a leg that would
+overrun it is skipped and says so in the JSON line.
 
 Workloads (seeded synthetic; no public dataset exists for this path):
   batched  9 species / 21 reactions, 1,048,576 cells, 20 % near ignition and
