@@ -47,3 +47,24 @@ def test_planted_error_is_not_explained(small):
     assert pu.explain(t, inp, g, bad, 1e-7, dict(atol=1e-15), tries=4).tolist() == [5]
     with pytest.raises(AssertionError):
         pu.check(t, inp, g, ref, 1e-7, dict(atol=1e-15), "planted")
+
+
+def test_reference_answers_on_indistinguishable_inputs_are_explained(small):
+    """The criterion's calibration, on the benchmarked cells at the bench's
+    options: oracle answers from one-ulp perturbations outside explain()'s
+    own tries (the reference's algorithm on inputs indistinguishable from the
+    cells' own) stand in for the GPU's answer, and every one of their cells
+    outside the tolerance is explained."""
+    import os
+    g0 = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "batched_ref.npz"))
+    t = small["tables"]
+    inp = (g0["in_T"], g0["in_p"], g0["in_rho"], g0["in_Y"])
+    dt = float(g0["dt"])
+    opts = dict(atol=1e-11, rtol=1e-4)
+    ref = {"T": g0["out_T"], "rho": g0["out_rho"], "Y": g0["out_Y"]}
+    for k in (1017, 1023):
+        Tk, Yk = pu.perturbations(inp[0], inp[3], k)
+        g = pu.oracle(t, Tk, inp[1], inp[2], Yk, dt, **opts)
+        bad = pu.bad_cells(g, ref)
+        assert bad.size > 0      # the sample has cells that one ulp moves
+        assert pu.explain(t, inp, g, bad, dt, opts, ref=ref).size == 0
