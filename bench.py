@@ -64,9 +64,10 @@ L2_FLUSH_BYTES = 256 << 20
 SUR_STEPS = 3            # timed gated-surrogate steps (fixed, whatever --steps)
 # DRAM bytes (read + write) per cell of one integrator launch on the 9-species
 # mechanism: ncu dram__bytes_read.sum + dram__bytes_write.sum of
-# integrate_kernel<10,32> over 5328 cells (profiles/integrator_group_kernel_small.md),
-# divided by the cells; the traffic grows with the cells integrated
-DRAM_BYTES_PER_CELL = {9: 817640.0 / 5328.0}
+# integrate_w_kernel<10> over 37,888 batched cells (4.840704 + 1.688320 MB,
+# profiles/integrator_warp_per_cell_batched.md), divided by the cells; the
+# traffic grows with the cells integrated
+DRAM_BYTES_PER_CELL = {9: (4.840704e6 + 1.688320e6) / 37888.0}
 
 
 # ----------------------------------------------------------------------------- helpers
@@ -398,7 +399,8 @@ def run_ours(args, ws, rank, local):
                          "traffic": (DRAM_BYTES_PER_CELL[nsp] * n if nsp in DRAM_BYTES_PER_CELL
                                      else None),
                          "traffic_note": "DRAM bytes per launch, scaled from an ncu capture "
-                                         "of 5328 cells by the cell count",
+                                         "of the warp-per-cell kernel on 37,888 cells by the "
+                                         "cell count",
                          "peak_source": "FP64 FMA probe measured in this run "
                                         "(no FP64 figure in the measured peaks file)",
                          "kernel_ms": kernel_ms, "flops_per_launch": flops_per_launch},
