@@ -13,11 +13,12 @@
 //    product of the species' exp(+-G0/(Ru T))), q, dq/dT, the third-body /
 //    fall-off factor and dq/dc of each participant, and writes them as a
 //    record to shared memory;
-//  * rows: lane i walks the list of reactions species i takes part in
-//    (mechanism order) and sums its row of f and of the Jacobian (the row in
-//    shared memory, the columns the reaction's participants), the
-//    temperature column entry and its entry of the temperature row
-//    (sum_r dH_r dq_r/dc_i, dH_r = sum nu h);
+//  * rows: lanes i and i + 16 walk the list of reactions species i takes
+//    part in (mechanism order; the even entries and the odd ones) and sum
+//    its row of f and of the Jacobian (rows in shared memory, the columns
+//    the reaction's participants), the temperature column entry and its
+//    entry of the temperature row (sum_r dH_r dq_r/dc_i, dH_r = sum nu h);
+//    the two partial sums are then added;
 //  * LU: lane i holds row i of I - dt J in registers; partial pivoting picks
 //    the first largest |a(k)| in the current row order (a warp argmax) and
 //    broadcasts the pivot row by shuffles; rows are never moved, each lane
@@ -87,7 +88,8 @@ struct WSmem {
     static constexpr int LD = (N % 2 == 0) ? N + 1 : N;
     static constexpr int kSV = 0;              // c, h, E, R, g, dgt: 6 x 32
     static constexpr int kJ = kSV + 6 * 32;    // rows of J, N x LD
-    static constexpr int kRec = kJ + N * LD;   // records, kWRec x nrc32, then the exponentials (njob32)
+    static constexpr int kJ2 = kJ + N * LD;    // the second half-warp's partial rows of J
+    static constexpr int kRec = kJ2 + N * LD;  // records, kWRec x nrc32, then the exponentials (njob32)
     __host__ __device__ static size_t doubles(int nrc32, int njob32) { return (size_t)kRec + kWRec * (size_t)nrc32 + njob32; }
     static size_t bytes(int nrc32, int njob32) { return sizeof(double) * doubles(nrc32, njob32); }
 };
@@ -212,15 +214,17 @@ struct WCtx {
         // ---- rows of f and J
         double f = 0.0, jt = 0.0, S = 0.0;
         double *Jrow = s + SM::kJ + lane * SM::LD;
-        // rows of the species (lane < nsp) and of padding species between them
-        // and T (zero rows: identity rows of I - dt J)
-        if (jac && lane < N - 1) {
+        // species i's entries are split between lanes i (even entries) and
+        // i + 16 (odd entries, into a partial row), then summed
+        const int hi = lane >> 4, sl = lane & 15;
+        double *Jp = hi ? s + SM::kJ2 + sl * SM::LD : Jrow;
+        if (jac && sl < N - 1) {
 #pragma unroll
-            for (int j = 0; j < N; ++j) Jrow[j] = 0.0;
+            for (int j = 0; j < N; ++j) Jp[j] = 0.0;
         }
-        if (lane < nsp) {
-            const int e0 = tb.lptr[lane], e1 = tb.lptr[lane + 1];
-            for (int e = e0; e < e1; ++e) {
+        if (sl < nsp) {
+            const int e0 = tb.lptr[sl], e1 = tb.lptr[sl + 1];
+            for (int e = e0 + hi; e < e1; e += 2) {
                 const int w0 = tb.lent[3 * e];
                 const int r = w0 & 0xffff, pos = (w0 >> 16) & 7, np = (w0 >> 20) & 15;
                 const double *R = recp(r);
@@ -234,21 +238,32 @@ struct WCtx {
                 for (int k = 0; k < 8; ++k) {
                     if (k >= np) break;
                     const int col = ((k < 4 ? c0 : c1) >> (8 * (k & 3))) & 0xff;
-                    Jrow[col] += nu * R[(4 + k) * 32];
+                    Jp[col] += nu * R[(4 + k) * 32];
                 }
                 if (w0 & (1 << 24)) {
                     const double gn = nu * R[2 * 32];
                     const double *er = &tb.eff[(size_t)r * nsp];
-                    for (int j = 0; j < nsp; ++j) Jrow[j] += er[j] * gn;
+                    for (int j = 0; j < nsp; ++j) Jp[j] += er[j] * gn;
                 }
             }
             if (jac) {
                 // the temperature row's third-body / fall-off columns
-                for (int t = 0; t < m.ntb; ++t) {
+                for (int t = hi; t < m.ntb; t += 2) {
                     const int r = tb.tbl[t];
                     const double *R = recp(r);
-                    S += R[3 * 32] * (tb.eff[(size_t)r * nsp + lane] * R[2 * 32]);
+                    S += R[3 * 32] * (tb.eff[(size_t)r * nsp + sl] * R[2 * 32]);
                 }
+            }
+        }
+        f += __shfl_xor_sync(full, f, 16);
+        if (jac) {
+            jt += __shfl_xor_sync(full, jt, 16);
+            S += __shfl_xor_sync(full, S, 16);
+            __syncwarp();
+            if (lane < nsp) {
+                const double *J2 = s + SM::kJ2 + lane * SM::LD;
+#pragma unroll
+                for (int j = 0; j < N - 1; ++j) Jrow[j] += J2[j];
             }
         }
         // ---- temperature equation (constant pressure, chemistrySource.cpp:863-883, 991-1021)
