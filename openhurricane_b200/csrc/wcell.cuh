@@ -1,5 +1,5 @@
 // Warp-per-cell implicit-Euler integrator (kernel 6) for mechanisms of
-// N = nsp + 1 <= 32 unknowns, FP64.
+// N = nsp + 1 <= 16 unknowns, FP64.
 //
 // One warp integrates one cell at a time and takes the next cell from the
 // device work queue (the grid is persistent). The per-cell control flow is
@@ -20,7 +20,8 @@
 //    entry of the temperature row (sum_r dH_r dq_r/dc_i, dH_r = sum nu h);
 //    the two partial sums are then added;
 //  * LU: lane i holds row i of I - dt J in registers; partial pivoting picks
-//    the first largest |a(k)| in the current row order (a warp argmax) and
+//    the first largest |a(k)| in the current row order (warp max reductions
+//    of its bit pattern, then a min reduction of the logical position) and
 //    broadcasts the pivot row by shuffles; rows are never moved, each lane
 //    keeps its logical position;
 //  * the triangular solves run along the logical order with shuffles.
@@ -440,21 +441,19 @@ struct WCtx {
         // in the current logical order on ties (LUDecomposeDPivoting)
 #pragma unroll
         for (int k = 0; k < N; ++k) {
-            double v = (lane < N && lpos >= k) ? fabs(a[k]) : -1.0;
-            int key = (lpos << 5) | lane;
-            // rows live in lanes < N: the butterfly spans the smallest power of
-            // two covering them (lanes above it reduce among themselves, unused)
-#pragma unroll
-            for (int o = (N > 16) ? 16 : (N > 8) ? 8 : (N > 4) ? 4 : (N > 2) ? 2 : 1; o > 0; o >>= 1) {
-                const double w = __shfl_xor_sync(full, v, o);
-                const int kw = __shfl_xor_sync(full, key, o);
-                if (w > v || (w == v && kw < key)) {
-                    v = w;
-                    key = kw;
-                }
-            }
-            const int pl = key & 31;          // pivot lane
-            const int pos_p = key >> 5;       // its logical position
+            // the largest |a(k)| by warp reductions of its bit pattern (a
+            // non-negative double orders like its bits; NaN never wins), then
+            // the first such row in the logical order
+            const double av = fabs(a[k]);
+            const bool cand = lane < N && lpos >= k;
+            const unsigned long long bits = (cand && av == av) ? (unsigned long long)__double_as_longlong(av) : 0ull;
+            const unsigned hi = (unsigned)(bits >> 32), lo = (unsigned)bits;
+            const unsigned mhi = __reduce_max_sync(full, hi);
+            const unsigned mlo = __reduce_max_sync(full, (hi == mhi) ? lo : 0u);
+            const unsigned kb = (cand && hi == mhi && lo == mlo) ? (unsigned)((lpos << 5) | lane) : 0xffffffffu;
+            const unsigned key = __reduce_min_sync(full, kb);
+            const int pl = (int)(key & 31);          // pivot lane
+            const int pos_p = (int)(key >> 5);       // its logical position
             // the rows swap logical positions k and pos_p
             if (lane == pl) lpos = k;
             else if (lpos == k) lpos = pos_p;
