@@ -344,10 +344,13 @@ def run_ours(args, ws, rank, local):
     step_s = ms_local / args.steps * 1e-3
     sur = None
     if args.surrogate and name == "batched":
-        # fixed work, whatever --steps: sample generation (FP64 integrations
-        # of sur_samples cells), training, and SUR_STEPS timed gated steps
-        # (at worst every cell rejected: a plain step each)
-        est = step_s * (args.sur_samples / n + SUR_STEPS + 1) + 2e-6 * args.sur_epochs * args.sur_samples
+        # fixed work, whatever --steps: sample generation (two FP64
+        # integrations of sur_samples cells: 0.74 plain steps for 524,288
+        # samples on the 1,048,576-cell workload), training (13.4 s for 150
+        # epochs of 524,288 samples) and SUR_STEPS + 1 gated steps (0.41 of
+        # a plain step each at a 29 % reject rate); with margins
+        est = (step_s * (1.5 * args.sur_samples / n + 0.6 * (SUR_STEPS + 1)) +
+               3e-7 * args.sur_epochs * args.sur_samples)
         if elapsed() + est > args.budget_s - 60:
             sur = {"skipped": f"wall-clock budget: needs about {est:.0f} s, "
                               f"{args.budget_s - elapsed():.0f} s left of --budget-s {args.budget_s:g}"}
