@@ -64,10 +64,10 @@ L2_FLUSH_BYTES = 256 << 20
 SUR_STEPS = 3            # timed gated-surrogate steps (fixed, whatever --steps)
 # DRAM bytes (read + write) per cell of one integrator launch on the 9-species
 # mechanism: ncu dram__bytes_read.sum + dram__bytes_write.sum of
-# integrate_w_kernel<10> over 37,888 batched cells (4.840704 + 1.688320 MB,
+# integrate_w_kernel<10> over 37,888 batched cells (4.971776 + 2.029312 MB,
 # profiles/integrator_warp_per_cell_batched.md), divided by the cells; the
 # traffic grows with the cells integrated
-DRAM_BYTES_PER_CELL = {9: (4.840704e6 + 1.688320e6) / 37888.0}
+DRAM_BYTES_PER_CELL = {9: (4.971776e6 + 2.029312e6) / 37888.0}
 
 
 # ----------------------------------------------------------------------------- helpers

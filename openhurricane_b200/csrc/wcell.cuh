@@ -13,12 +13,13 @@
 //    product of the species' exp(+-G0/(Ru T))), q, dq/dT, the third-body /
 //    fall-off factor and dq/dc of each participant, and writes them as a
 //    record to shared memory;
-//  * rows: lanes i and i + 16 walk the list of reactions species i takes
-//    part in (mechanism order; the even entries and the odd ones) and sum
-//    its row of f and of the Jacobian (rows in shared memory, the columns
-//    the reaction's participants), the temperature column entry and its
-//    entry of the temperature row (sum_r dH_r dq_r/dc_i, dH_r = sum nu h);
-//    the two partial sums are then added;
+//  * rows: lanes i, i + 11 and i + 22 (N <= 11; i and i + 16 above) walk
+//    the list of reactions species i takes part in (mechanism order; every
+//    third or second entry each) and sum its row of f and of the Jacobian
+//    (rows in shared memory, the columns the reaction's participants), the
+//    temperature column entry and its entry of the temperature row
+//    (sum_r dH_r dq_r/dc_i, dH_r = sum nu h); the partial sums are then
+//    added in lane order;
 //  * LU: lane i holds row i of I - dt J in registers; partial pivoting picks
 //    the first largest |a(k)| in the current row order (warp max reductions
 //    of its bit pattern, then a min reduction of the logical position) and
@@ -89,8 +90,9 @@ struct WSmem {
     static constexpr int LD = (N % 2 == 0) ? N + 1 : N;
     static constexpr int kSV = 0;              // c, h, E, R, g, dgt: 6 x 32
     static constexpr int kJ = kSV + 6 * 32;    // rows of J, N x LD
-    static constexpr int kJ2 = kJ + N * LD;    // the second half-warp's partial rows of J
-    static constexpr int kRec = kJ2 + N * LD;  // records, kWRec x nrc32, then the exponentials (njob32)
+    static constexpr int kW = (N <= 11) ? 3 : 2;   // lanes per species row
+    static constexpr int kJ2 = kJ + N * LD;    // the other lanes' partial rows of J
+    static constexpr int kRec = kJ2 + (kW - 1) * N * LD;  // records, kWRec x nrc32, then the exponentials (njob32)
     __host__ __device__ static size_t doubles(int nrc32, int njob32) { return (size_t)kRec + kWRec * (size_t)nrc32 + njob32; }
     static size_t bytes(int nrc32, int njob32) { return sizeof(double) * doubles(nrc32, njob32); }
 };
@@ -215,17 +217,19 @@ struct WCtx {
         // ---- rows of f and J
         double f = 0.0, jt = 0.0, S = 0.0;
         double *Jrow = s + SM::kJ + lane * SM::LD;
-        // species i's entries are split between lanes i (even entries) and
-        // i + 16 (odd entries, into a partial row), then summed
-        const int hi = lane >> 4, sl = lane & 15;
-        double *Jp = hi ? s + SM::kJ2 + sl * SM::LD : Jrow;
+        // species i's entries are split between lanes i, i + WS (and i + 2 WS):
+        // entry e goes to the (e - e0) mod kW-th of them, the others' partial
+        // rows are added to lane i's
+        constexpr int WS = (SM::kW == 3) ? 11 : 16;   // lane stride between a row's workers
+        const int hi = lane / WS, sl = lane - WS * hi;
+        double *Jp = hi ? s + SM::kJ2 + (hi - 1) * N * SM::LD + sl * SM::LD : Jrow;
         if (jac && sl < N - 1) {
 #pragma unroll
             for (int j = 0; j < N; ++j) Jp[j] = 0.0;
         }
         if (sl < nsp) {
             const int e0 = tb.lptr[sl], e1 = tb.lptr[sl + 1];
-            for (int e = e0 + hi; e < e1; e += 2) {
+            for (int e = e0 + hi; e < e1; e += SM::kW) {
                 const int w0 = tb.lent[3 * e];
                 const int r = w0 & 0xffff, pos = (w0 >> 16) & 7, np = (w0 >> 20) & 15;
                 const double *R = recp(r);
@@ -249,22 +253,37 @@ struct WCtx {
             }
             if (jac) {
                 // the temperature row's third-body / fall-off columns
-                for (int t = hi; t < m.ntb; t += 2) {
+                for (int t = hi; t < m.ntb; t += SM::kW) {
                     const int r = tb.tbl[t];
                     const double *R = recp(r);
                     S += R[3 * 32] * (tb.eff[(size_t)r * nsp + sl] * R[2 * 32]);
                 }
             }
         }
-        f += __shfl_xor_sync(full, f, 16);
-        if (jac) {
-            jt += __shfl_xor_sync(full, jt, 16);
-            S += __shfl_xor_sync(full, S, 16);
-            __syncwarp();
-            if (lane < nsp) {
-                const double *J2 = s + SM::kJ2 + lane * SM::LD;
+        if constexpr (SM::kW == 3) {
+            const int s1 = (lane + 11) & 31, s2 = (lane + 22) & 31;
+            f = (f + __shfl_sync(full, f, s1)) + __shfl_sync(full, f, s2);
+            if (jac) {
+                jt = (jt + __shfl_sync(full, jt, s1)) + __shfl_sync(full, jt, s2);
+                S = (S + __shfl_sync(full, S, s1)) + __shfl_sync(full, S, s2);
+                __syncwarp();
+                if (lane < nsp) {
+                    const double *J2 = s + SM::kJ2 + lane * SM::LD, *J3 = J2 + N * SM::LD;
 #pragma unroll
-                for (int j = 0; j < N - 1; ++j) Jrow[j] += J2[j];
+                    for (int j = 0; j < N - 1; ++j) Jrow[j] = (Jrow[j] + J2[j]) + J3[j];
+                }
+            }
+        } else {
+            f += __shfl_xor_sync(full, f, 16);
+            if (jac) {
+                jt += __shfl_xor_sync(full, jt, 16);
+                S += __shfl_xor_sync(full, S, 16);
+                __syncwarp();
+                if (lane < nsp) {
+                    const double *J2 = s + SM::kJ2 + lane * SM::LD;
+#pragma unroll
+                    for (int j = 0; j < N - 1; ++j) Jrow[j] += J2[j];
+                }
             }
         }
         // ---- temperature equation (constant pressure, chemistrySource.cpp:863-883, 991-1021)
