@@ -356,7 +356,7 @@ def run_ours(args, ws, rank, local):
                               f"{args.budget_s - elapsed():.0f} s left of --budget-s {args.budget_s:g}"}
     if args.surrogate and name == "batched" and sur is None:
         sur = surrogate_leg(args, wl, mech, (T0, p0, rho0, Y0), dt, fp64_ref,
-                            ms_local / args.steps, flush, rank)
+                            ms_local / args.steps, flush, rank, counters["n_newton"])
     if graph is not None:
         del graph
 
@@ -465,7 +465,7 @@ def properties_leg(mech, fields0, flush, prop_cells):
             "bytes_per_launch": nbytes}
 
 
-def surrogate_leg(args, wl, mech, fields0, dt, fp64_ref, plain_ms, flush, rank):
+def surrogate_leg(args, wl, mech, fields0, dt, fp64_ref, plain_ms, flush, rank, plain_newton):
     """Train the gated surrogate on samples of the FP64 GPU integrator (states
     of the same distribution, another seed), then time its flow step on the
     workload's cells and compare it with the FP64 step."""
@@ -512,7 +512,8 @@ def surrogate_leg(args, wl, mech, fields0, dt, fp64_ref, plain_ms, flush, rank):
         flush.fill_(float(k))
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        nr, accept = sur.step(flow, dt, opts=opts)
+        fb = {}
+        nr, accept = sur.step(flow, dt, opts=opts, counters=fb)
         b.record(stream)
         torch.cuda.synchronize()
         ms.append(a.elapsed_time(b))
@@ -528,6 +529,9 @@ def surrogate_leg(args, wl, mech, fields0, dt, fp64_ref, plain_ms, flush, rank):
     return {"cells_per_s": n / (sur_ms * 1e-3), "ms_per_step": sur_ms,
             "speedup_vs_plain": plain_ms / sur_ms,
             "reject_rate": float(np.mean(rej)) / n,
+            "fp64_work_gain": plain_newton / max(1, fb.get("n_newton", 0)),
+            "fp64_work_gain_note": "Newton iterations of the plain step / of the gated step's FP64 "
+                                   "fallback on the same cells",
             "max_abs_dT_K": float(dT.max()), "max_abs_dT_accepted_K": float(dT[acc].max()) if
             bool(acc.any()) else 0.0,
             "linf_dY": float(dY.max()),

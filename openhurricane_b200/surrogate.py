@@ -238,15 +238,18 @@ class Surrogate:
 
     # ------------------------------------------------------------------ infer
     def step(self, flow, dt: torch.Tensor, dt_factor: float = 1.0, opts=None,
-             subdt: Optional[torch.Tensor] = None):
+             subdt: Optional[torch.Tensor] = None, counters: Optional[dict] = None):
         """One gated surrogate flow step on `flow` (T, p, rho, Y updated in
-        place). Returns (n_rejected, accept mask)."""
+        place). Returns (n_rejected, accept mask). `counters`, when given, is
+        filled with the FP64 fallback's work counters (n_newton, ...; zeros
+        when no cell is rejected)."""
         n = flow.n
         X = self.features(flow.T, flow.p, flow.Y, dt, dt_factor)
         pred, spread = self.predict(X)
-        return self.apply(flow, dt, X, pred, spread, dt_factor, opts, subdt)
+        return self.apply(flow, dt, X, pred, spread, dt_factor, opts, subdt, counters)
 
-    def apply(self, flow, dt, X, pred, spread, dt_factor: float = 1.0, opts=None, subdt=None):
+    def apply(self, flow, dt, X, pred, spread, dt_factor: float = 1.0, opts=None, subdt=None,
+              counters: Optional[dict] = None):
         """The gate and the FP64 fallback for a given prediction."""
         n = flow.n
         accept = torch.empty(n, dtype=torch.int32, device=flow.T.device)
@@ -259,13 +262,16 @@ class Surrogate:
             _vp_stream()),
             "hc_surrogate_gate")
         nr = int(nrej.value)
+        cnt = _capi.HcCounters() if counters is not None else None
         if nr > 0:
             o = opts if opts is not None else _capi.default_opts()
             sub = subdt if subdt is not None else (dt * dt_factor).clone()
             _capi.check(_capi.load().hc_integrate_subset(
                 self.mech.handle, C.byref(o), n, nr, _vp(rejected), _vp(flow.T), _vp(flow.p),
                 _vp(flow.rho), _vp(flow.Y), _vp(dt), float(dt_factor), _vp(sub), None, None, None,
-                None, _vp_stream()), "hc_integrate_subset")
+                C.addressof(cnt) if cnt is not None else None, _vp_stream()), "hc_integrate_subset")
+        if counters is not None:
+            counters.update(cnt.as_dict())
         return nr, accept
 
 

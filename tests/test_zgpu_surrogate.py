@@ -28,8 +28,8 @@ def test_element_projector_conserves(small):
 
 def test_gated_surrogate_small_mechanism(small):
     from openhurricane_b200 import synth, workloads
-    from openhurricane_b200.chemistry import Flow, Mechanism
-    from openhurricane_b200.surrogate import Surrogate, generate_samples, integrate_device
+    from openhurricane_b200.chemistry import ChemistrySource, Flow, Mechanism
+    from openhurricane_b200.surrogate import Surrogate, generate_samples
     dev = torch.device("cuda:0")
     t = small["tables"]
     mech = Mechanism(t)
@@ -52,15 +52,25 @@ def test_gated_surrogate_small_mechanism(small):
     n = test.n
     ref = Flow(d(test.T), d(test.p), d(test.rho), d(test.Y))
     dt = torch.full((n,), 1e-5, dtype=torch.float64, device=dev)
-    integrate_device(mech, ref.T, ref.p, ref.rho, ref.Y, dt, opts)
+    # the method without the network: every cell by the FP64 integrator
+    plain = ChemistrySource(mech, ref, **workloads.SOLVER_OPTS)
+    plain.rebin = False
+    plain.solveUpdate(dt, 1.0, counters=True)
     flow = Flow(d(test.T), d(test.p), d(test.rho), d(test.Y))
     e0 = _element_mass(t, flow.Y)
-    nrej, accept = sur.step(flow, dt, opts=opts)
+    fallback = {}
+    nrej, accept = sur.step(flow, dt, opts=opts, counters=fallback)
     torch.cuda.synchronize()
     acc = accept.bool()
     dT = (flow.T - ref.T).abs()
-    print(f"rejected {nrej}/{n}, max|dT| accepted {dT[acc].max().item():.3f} K")
+    # what the network gains: the FP64 Newton iterations (each a Jacobian, an
+    # LU and a solve) the gated step leaves to the integrator, against the
+    # plain step's on the same cells
+    gain = plain.last_counters["n_newton"] / max(1, fallback["n_newton"])
+    print(f"rejected {nrej}/{n}, max|dT| accepted {dT[acc].max().item():.3f} K, "
+          f"FP64 work of the plain step / of the gated step's fallback = {gain:.2f}")
     assert nrej < n                     # the network takes part
+    assert gain > 1.5
     assert dT.max().item() < 5.0
     # rejected cells: the FP64 integrator's own result
     assert torch.equal(flow.T[~acc], ref.T[~acc])
