@@ -142,6 +142,22 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# ----------------------------------------------------------------------------- time budget
+def surrogate_leg_seconds(step_s: float, samples: int, ncells: int, epochs: int) -> float:
+    """Estimated wall time of the gated-surrogate leg: sample generation (two
+    FP64 integrations of `samples` cells: 0.74 plain steps for 524,288 samples
+    on the 1,048,576-cell workload), training (13.4 s for 150 epochs of
+    524,288 samples) and SUR_STEPS + 1 gated steps (0.41 of a plain step each
+    at a 29 % reject rate), with margins. Its sizes are fixed: --steps does
+    not enter."""
+    return step_s * (1.5 * samples / ncells + 0.6 * (SUR_STEPS + 1)) + 3e-7 * epochs * samples
+
+
+def fits_budget(elapsed_s: float, leg_s: float, budget_s: float, reserve_s: float = 60.0) -> bool:
+    """A leg runs only if it ends `reserve_s` before the wall-clock budget."""
+    return elapsed_s + leg_s <= budget_s - reserve_s
+
+
 # ----------------------------------------------------------------------------- workloads
 def build_workload(name: str, ncells: int, seed_offset: int):
     from openhurricane_b200 import workloads
@@ -344,14 +360,8 @@ def run_ours(args, ws, rank, local):
     step_s = ms_local / args.steps * 1e-3
     sur = None
     if args.surrogate and name == "batched":
-        # fixed work, whatever --steps: sample generation (two FP64
-        # integrations of sur_samples cells: 0.74 plain steps for 524,288
-        # samples on the 1,048,576-cell workload), training (13.4 s for 150
-        # epochs of 524,288 samples) and SUR_STEPS + 1 gated steps (0.41 of
-        # a plain step each at a 29 % reject rate); with margins
-        est = (step_s * (1.5 * args.sur_samples / n + 0.6 * (SUR_STEPS + 1)) +
-               3e-7 * args.sur_epochs * args.sur_samples)
-        if elapsed() + est > args.budget_s - 60:
+        est = surrogate_leg_seconds(step_s, args.sur_samples, n, args.sur_epochs)
+        if not fits_budget(elapsed(), est, args.budget_s):
             sur = {"skipped": f"wall-clock budget: needs about {est:.0f} s, "
                               f"{args.budget_s - elapsed():.0f} s left of --budget-s {args.budget_s:g}"}
     if args.surrogate and name == "batched" and sur is None:
